@@ -1,0 +1,372 @@
+"""Benchmark: R-MAT-22 PageRank (GTEPS and achieved HBM GB/s) on one B200.
+
+Workload (the reference's full plain-kernel configuration): R-MAT scale 22
+(4,194,304 nodes, edge factor 16, a/b/c/d = .57/.19/.19/.05, seed 2, self-loops
+and duplicate edges removed -> 65,243,929 directed edges), pull PageRank with
+damping 0.85, tol 1e-6 (L1), max_iter 100.  A step is one pagerank() call to
+convergence.  Inputs are synthetic (seeded generator; the reference publishes
+no dataset at this scale) and larger than L2 (the in-CSR alone is 261 MB), so
+no L2 flush is needed between steps.
+
+  value  GTEPS = edges x iterations / device time, topology resident in HBM,
+         through ursa_gpu_pagerank_device (events on the launch stream).
+  e2e    the same metric through the C ABI a caller uses, from pinned host
+         buffers: Topology::build (H2D of src/dst, CSR build, transpose) +
+         pagerank (D2H of the n f64 ranks) per step.
+  --impl reference
+         the reference algorithm on the host cores: the CPU restatement of
+         ursa-core (the Rust crate cannot be built here), same workload, all
+         host threads, one full build + transpose + pagerank per step.
+
+Multi-GPU (--gpus N under torchrun): replicas only (each rank runs the whole
+workload on its own GPU, no collective on the data path); value sums ranks'
+edges x iterations over the max time across ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE, EDGE_FACTOR, SEED = 22, 16, 2
+DAMPING, TOL, MAX_ITER = 0.85, 1e-6, 100
+WORKLOAD = "rmat22_pagerank"
+
+# dram__bytes_read.sum + dram__bytes_write.sum of one pr_persistent_k launch on
+# this workload, from the ncu capture summarised in
+# profiles/pagerank_rmat22.md (None until captured).
+NCU_TRAFFIC = None  # {"bytes_per_launch": B, "iterations": I}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def algorithmic_bytes(n: int, m: int, iters: int) -> int:
+    """Compulsory HBM bytes of one pagerank launch.
+
+    Per iteration: in-CSR sources 4m, in-CSR offsets 4(n+1), the f32 share of
+    each node gathered at least once 4n, old rank 8n, out-degree 4n, new rank
+    8n, new share 4n  ->  4m + 32n + 4.  Prologue: out-degree 4n, rank 8n,
+    share 4n  ->  16n.
+    """
+    return iters * (4 * m + 32 * n + 4) + 16 * n
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+        rows = [r for r in self.rows if self.uuid is None or self.uuid in r[0]]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_workload():
+    from ursa_b200 import gen
+
+    n, src, dst = gen.rmat(SCALE, EDGE_FACTOR, SEED)
+    return n, src, dst
+
+
+def run_reference(args, rank, world):
+    """The reference algorithm on the host (CPU restatement of ursa-core)."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    n, src, dst = make_workload()
+    m = int(src.size)
+
+    def step():
+        t0 = time.perf_counter()
+        topo = O.Topology(n, src, dst)
+        _, it = O.pagerank(topo, DAMPING, MAX_ITER, TOL, return_iters=True)
+        dt = time.perf_counter() - t0
+        del topo
+        return dt, it
+
+    for _ in range(args.warmup):
+        step()
+    times, iters = [], []
+    for _ in range(args.steps):
+        dt, it = step()
+        times.append(dt)
+        iters.append(it)
+    total = sum(times)
+    value = m * sum(iters) / total / 1e9
+    line = {
+        "impl": "reference",
+        "metric": "pagerank_gteps",
+        "value": value,
+        "unit": "GTEPS",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": TOL,
+                   "max_iter": MAX_ITER, "iterations": iters[-1], "l2": "inputs larger than L2",
+                   "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "port",
+                         "sample": "full Topology::build + transpose + pagerank to tol per step "
+                                   "(C restatement of ursa-core; the Rust crate cannot be built here)"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(n, src, dst):
+    """Warm CPU PageRank GTEPS of the oracle on this workload (bounded sample:
+    5 fixed power iterations with the CSR and transpose prebuilt)."""
+    from oracle import oracle as O
+
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    topo = O.Topology(n, src, dst)
+    topo.csr("in")  # prebuild the transpose (warm kernel)
+    iters = 5
+    t0 = time.perf_counter()
+    O.pagerank(topo, DAMPING, iters, 0.0)
+    dt = time.perf_counter() - t0
+    return {"value": src.size * iters / dt / 1e9, "unit": "GTEPS", "cores": threads, "kind": "port",
+            "sample": f"{iters} warm power iterations (tol=0) on the same R-MAT-22 graph, CSR+transpose prebuilt"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local_rank = env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    from ursa_b200 import PageRankParams, PageRankStats, Topology, _lib
+
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(local_rank))
+    n, src, dst = make_workload()
+    m = int(src.size)
+    params = PageRankParams(DAMPING, MAX_ITER, TOL)
+
+    # ---- value: topology resident, device output
+    topo = Topology.build(n, src, dst)
+    topo.prepare(transpose=True)
+    stream = torch.cuda.Stream()
+    d_out = torch.empty(n, dtype=torch.float64, device="cuda")
+
+    def dev_step(st):
+        _lib.check(L.ursa_gpu_pagerank_device(topo.handle, C.byref(params), d_out.data_ptr(),
+                                              C.c_void_p(stream.cuda_stream), C.byref(st)))
+
+    for _ in range(max(args.warmup, 3)):
+        dev_step(PageRankStats())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    launches0 = L.ursa_gpu_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stats = []
+    for i in range(args.steps):
+        st = PageRankStats()
+        ev[i][0].record(stream)
+        dev_step(st)
+        ev[i][1].record(stream)
+        stats.append(st)
+    torch.cuda.synchronize()
+    launches = L.ursa_gpu_launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    edges_iters = sum(m * s.iterations for s in stats)
+    kernel_ms = [s.device_ms for s in stats]
+
+    # ---- e2e: the C-ABI call from pinned host buffers (build + pagerank)
+    h_src = torch.from_numpy(src).pin_memory()
+    h_dst = torch.from_numpy(dst).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float64).pin_memory()
+    ps, pd, po = h_src.data_ptr(), h_dst.data_ptr(), h_out.data_ptr()
+
+    def e2e_step():
+        h = C.c_void_p()
+        st = PageRankStats()
+        _lib.check(L.ursa_gpu_topo_build(n, ps, pd, m, C.byref(h)))
+        try:
+            _lib.check(L.ursa_gpu_pagerank(h, C.byref(params), po, C.byref(st)))
+        finally:
+            L.ursa_gpu_topo_free(h)
+        return st.iterations
+
+    for _ in range(max(min(args.warmup, 2), 1)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_times, e2e_iters = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        it = e2e_step()
+        e2e_times.append(time.perf_counter() - t0)
+        e2e_iters.append(it)
+    clocks = sampler.stop() if sampler else None
+
+    # ---- max over ranks
+    t_dev = total_ms
+    t_e2e = sum(e2e_times)
+    if dist:
+        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(tt[0]), float(tt[1])
+        ei = torch.tensor([float(edges_iters), float(m * sum(e2e_iters))], dtype=torch.float64, device="cuda")
+        dist.all_reduce(ei, op=dist.ReduceOp.SUM)
+        edges_iters_all, e2e_edges_all = float(ei[0]), float(ei[1])
+    else:
+        edges_iters_all, e2e_edges_all = float(edges_iters), float(m * sum(e2e_iters))
+
+    if rank == 0:
+        iters = stats[-1].iterations
+        mean_kernel_ms = sum(kernel_ms) / len(kernel_ms)
+        alg = algorithmic_bytes(n, m, iters)
+        achieved = alg / (mean_kernel_ms * 1e-3) / 1e9
+        peak, peak_kind = load_peaks()
+        traffic = None
+        if NCU_TRAFFIC:
+            per_iter = NCU_TRAFFIC["bytes_per_launch"] / max(NCU_TRAFFIC["iterations"], 1)
+            traffic = per_iter * iters
+        line = {
+            "metric": "pagerank_gteps",
+            "value": edges_iters_all / (t_dev * 1e-3) / 1e9,
+            "unit": "GTEPS",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t_dev / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32-compensated SpMV, f64 ranks/residual",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": TOL,
+                       "max_iter": MAX_ITER, "iterations": iters, "l2": "inputs larger than L2 (in-CSR 261 MB)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": {"value": e2e_edges_all / t_e2e / 1e9, "unit": "GTEPS",
+                    "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * n,
+                    "ms_per_step": 1e3 * t_e2e / args.steps},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "kernel": "pr_persistent_k", "kernel_ms": mean_kernel_ms,
+                         "algorithmic_bytes_per_launch": alg},
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(n, src, dst)
+        print(json.dumps(line), flush=True)
+    del topo
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/*
+ * ursa_gpu.h -- C ABI of the B200 (sm_100a) implementation of ursa-core's CSR
+ * topology and graph kernels (cldixon/ursa, ursa-core/src).
+ *
+ * Each entry point replaces one public function of ursa-core; the comment on
+ * each names the Rust item (file:line, paths relative to the ursa project
+ * root) whose meaning, argument order and edge-case behaviour it keeps.  A
+ * Rust FFI crate binds these declarations one-to-one; the kernel functions'
+ * Rust bodies call them and keep their signatures, so GraphAlgorithmExec
+ * (ursa-plan/src/physical.rs:40) and the PyO3 layer see no change.
+ *
+ * Conventions
+ *  - Node ids are uint32; host-visible CSR offsets are uint64, as in
+ *    Adjacency (ursa-core/src/topology.rs:36-47).
+ *  - direction: 0 = Out, 1 = In, 2 = Both (topology.rs:28-32).
+ *  - Weights are f64 indexed by ORIGINAL edge row, length == n_edges
+ *    (pagerank.rs:140-144); they must be non-negative (validated upstream by
+ *    ursa-plan/src/weight.rs:51-106).
+ *  - Every function returns URSA_GPU_OK (0) or an error status; the message
+ *    of the last error on the calling thread is ursa_gpu_last_error().  The
+ *    Rust shim maps a non-OK status to panic!, which the plan layer already
+ *    turns into a DataFusionError (physical.rs:106-108).
+ *  - Host buffers are caller-allocated.  All calls are re-entrant: each host
+ *    thread gets its own CUDA stream, and a topology's lazily built parts
+ *    (transpose, undirected CSR) are created once under a mutex, like the
+ *    OnceLock fields of Topology (topology.rs:258-260).
+ */
+#ifndef URSA_GPU_H
+#define URSA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  URSA_GPU_OK = 0,
+  URSA_GPU_EINVAL = 1,   /* contract violation (the Rust code would assert!) */
+  URSA_GPU_ENOMEM = 2,   /* device memory / admission budget exhausted */
+  URSA_GPU_ECUDA = 3,    /* CUDA runtime error */
+  URSA_GPU_ETIMEOUT = 4, /* a bounded device-side wait expired */
+  URSA_GPU_ETRUNC = 5,   /* caller buffer too small; required size reported */
+  URSA_GPU_ENODEV = 6    /* no usable CUDA device */
+};
+
+typedef struct ursa_gpu_topo ursa_gpu_topo;
+typedef struct ursa_gpu_pairs ursa_gpu_pairs;
+
+/* Message for the last non-OK status returned on this thread. */
+const char *ursa_gpu_last_error(void);
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int ursa_gpu_version(void);
+/* Diagnostics, not part of ursa-core's surface: the number of kernels this
+ * library has launched in the process so far (benchmarks difference it
+ * around a timed region). */
+uint64_t ursa_gpu_launch_count(void);
+/* Selects the CUDA device used by topologies built afterwards on this thread. */
+int ursa_gpu_set_device(int device);
+
+/* ---- Topology (ursa-core/src/topology.rs) ------------------------------ */
+
+/* Topology::build(n_nodes, src_dense, dst_dense) -- topology.rs:276-298.
+ * Host arrays of n_edges endpoints, each < n_nodes.  Copies to the device and
+ * builds the out-CSR by a stable counting sort (row order kept within each
+ * node's segment: byte-identical to Adjacency::build, topology.rs:54-187).
+ * n_edges > UINT32_MAX is rejected (topology.rs:61-65). */
+int ursa_gpu_topo_build(uint64_t n_nodes, const uint32_t *src, const uint32_t *dst,
+                        uint64_t n_edges, ursa_gpu_topo **out);
+/* Same as ursa_gpu_topo_build with device-resident endpoint arrays, enqueued
+ * on `stream` (a cudaStream_t, or NULL for this thread's stream).  Used by the
+ * serving layer, whose uploads already live in HBM. */
+int ursa_gpu_topo_build_device(uint64_t n_nodes, const uint32_t *d_src, const uint32_t *d_dst,
+                               uint64_t n_edges, void *stream, ursa_gpu_topo **out);
+/* Drop for Topology: frees every device buffer. NULL is a no-op. */
+void ursa_gpu_topo_free(ursa_gpu_topo *t);
+/* Topology::n_nodes / n_edges -- topology.rs:324-331. */
+uint64_t ursa_gpu_topo_n_nodes(const ursa_gpu_topo *t);
+uint64_t ursa_gpu_topo_n_edges(const ursa_gpu_topo *t);
+/* Topology::out() / incoming() -- topology.rs:335-348.  dir 0 = out-CSR,
+ * 1 = in-CSR (the transpose, built on first use from the out-CSR by
+ * reconstructing original row order, topology.rs:307-321).  Copies the pub
+ * fields offsets[n+1], targets[m], edge_ids[m] to host; NULL skips a field. */
+int ursa_gpu_topo_adjacency(ursa_gpu_topo *t, int dir, uint64_t *offsets, uint32_t *targets,
+                            uint32_t *edge_ids);
+/* Topology::undirected() -- topology.rs:353-389: out ∪ in per node, self-loops
+ * dropped, sorted, deduplicated.  *len receives targets.len(). */
+int ursa_gpu_topo_undirected_len(ursa_gpu_topo *t, uint64_t *len);
+int ursa_gpu_topo_undirected(ursa_gpu_topo *t, uint64_t *offsets, uint32_t *targets);
+/* Builds the lazily cached parts now (1 = transpose, 2 = undirected CSR,
+ * 3 = both).  Lets a caller move build cost out of a latency-critical call. */
+int ursa_gpu_topo_prepare(ursa_gpu_topo *t, int what);
+/* Device bytes held by the topology (CSRs plus cached plans). */
+uint64_t ursa_gpu_topo_device_bytes(const ursa_gpu_topo *t);
+
+/* ---- Kernels (ursa-core/src/algo, re-exported at algo/mod.rs:35-50) ---- */
+
+/* degree(&Topology, Direction) -> Vec<u32> -- algo/degree.rs:12-30. */
+int ursa_gpu_degree(ursa_gpu_topo *t, int dir, uint32_t *out);
+
+/* PageRankParams -- algo/pagerank.rs:22-36 (defaults 0.85 / 30 / 1e-6). */
+typedef struct {
+  double damping;
+  uint32_t max_iter;
+  double tol;
+} ursa_gpu_pagerank_params;
+
+/* Optional run statistics (not part of the Rust signature). */
+typedef struct {
+  uint32_t iterations;   /* power iterations executed */
+  double last_delta;     /* L1 residual of the last iteration */
+  double device_ms;      /* device time of the iteration kernel */
+} ursa_gpu_pagerank_stats;
+
+/* pagerank(&Topology, PageRankParams) -> Vec<f64> -- algo/pagerank.rs:98-124.
+ * Pull iteration over the in-CSR; the per-edge shares rank[v]/outdeg[v] are
+ * gathered in f32 and summed per row with compensated (TwoSum) f32
+ * accumulation; base term, dangling mass, L1 residual and the ranks stay
+ * f64.  No final renormalisation (as in power_iterate, pagerank.rs:63-94).
+ * out: n f64 (host).  stats may be NULL. */
+int ursa_gpu_pagerank(ursa_gpu_topo *t, const ursa_gpu_pagerank_params *params, double *out,
+                      ursa_gpu_pagerank_stats *stats);
+/* Device-output form of ursa_gpu_pagerank: d_out is an n-f64 device array,
+ * enqueued on `stream` (NULL = this thread's stream); returns after the
+ * kernel completes. */
+int ursa_gpu_pagerank_device(ursa_gpu_topo *t, const ursa_gpu_pagerank_params *params,
+                             double *d_out, void *stream, ursa_gpu_pagerank_stats *stats);
+/* pagerank_weighted(&Topology, &[f64], PageRankParams) -> Vec<f64> --
+ * algo/pagerank.rs:135-169.  weights: n_edges f64 by original edge row. */
+int ursa_gpu_pagerank_weighted(ursa_gpu_topo *t, const double *weights, uint64_t n_weights,
+                               const ursa_gpu_pagerank_params *params, double *out,
+                               ursa_gpu_pagerank_stats *stats);
+
+/* bfs_distances(&Topology, u32, Direction) -> Vec<i32> -- algo/bfs.rs:18-42.
+ * -1 = unreachable; out-of-range source gives all -1.  Direction-optimising
+ * (top-down / bottom-up) on the device; levels are exact. */
+int ursa_gpu_bfs_distances(ursa_gpu_topo *t, uint32_t source, int dir, int32_t *out);
+
+/* shortest_path(&Topology, u32, u32, Direction) -> Option<Vec<u32>> --
+ * algo/bfs.rs:48-102.  Writes the inclusive node path into path[0..cap) and
+ * its length into *len (-1 = None).  The parent of each node is its first
+ * discoverer in the reference's serial frontier order, so the path is the
+ * reference's path.  If the path is longer than cap: URSA_GPU_ETRUNC with
+ * *len set. */
+int ursa_gpu_shortest_path(ursa_gpu_topo *t, uint32_t source, uint32_t target, int dir,
+                           uint32_t *path, uint64_t cap, int64_t *len);
+
+/* dijkstra_distances(&Topology, &[f64], u32, Direction) -> Vec<f64> --
+ * algo/bfs.rs:126-166.  +inf = unreachable.  Distances are the same f64
+ * values Dijkstra settles (min over paths of the left-to-right f64 sums). */
+int ursa_gpu_dijkstra_distances(ursa_gpu_topo *t, const double *weights, uint64_t n_weights,
+                                uint32_t source, int dir, double *out);
+
+/* shortest_path_weighted_with_cost(...) -> Option<(Vec<u32>, Vec<f64>)> --
+ * algo/bfs.rs:192-259; shortest_path_weighted (bfs.rs:176-184) is this with
+ * costs == NULL.  path/costs have room for cap entries; *len = -1 for None. */
+int ursa_gpu_shortest_path_weighted_with_cost(ursa_gpu_topo *t, const double *weights,
+                                              uint64_t n_weights, uint32_t source,
+                                              uint32_t target, int dir, uint32_t *path,
+                                              double *costs, uint64_t cap, int64_t *len);
+
+/* k_hop(&Topology, &[u32], u32, Direction) -> (Vec<u32>, Vec<u32>) --
+ * algo/hop.rs:52-75.  Pairs are emitted per seed in seed order and, within a
+ * seed, in the reference's discovery order.  The result object owns the
+ * pairs: read them with ursa_gpu_pairs_len / _copy and release it with
+ * ursa_gpu_pairs_free. */
+int ursa_gpu_k_hop(ursa_gpu_topo *t, const uint32_t *seeds, uint64_t n_seeds, uint32_t k,
+                   int dir, ursa_gpu_pairs **out);
+uint64_t ursa_gpu_pairs_len(const ursa_gpu_pairs *p);
+int ursa_gpu_pairs_copy(const ursa_gpu_pairs *p, uint32_t *seeds_out, uint32_t *reached_out);
+void ursa_gpu_pairs_free(ursa_gpu_pairs *p);
+
+/* connected_components_weak(&Topology) -> Vec<u32> -- algo/components.rs:58-68.
+ * Labels are the minimum member id of each weak component (a valid
+ * "representative id" labelling; the reference's union-find picks another
+ * representative, and the partition is identical). */
+int ursa_gpu_connected_components_weak(ursa_gpu_topo *t, uint32_t *out);
+
+/* triangle_count(&Topology) -> Vec<u32> -- algo/triangle.rs:40-62: triangles
+ * through each node of the undirected simple view. */
+int ursa_gpu_triangle_count(ursa_gpu_topo *t, uint32_t *out);
+
+/* clustering_coefficient(&Topology) -> Vec<f64> -- algo/clustering.rs:21-40. */
+int ursa_gpu_clustering_coefficient(ursa_gpu_topo *t, double *out);
+
+/* betweenness(&Topology, Option<f64>, Option<u64>) -> Vec<f64> --
+ * algo/betweenness.rs:153-177.  has_sample/has_seed encode the Options.  The
+ * sampled source set is the reference's seeded shuffled_order prefix
+ * (betweenness.rs:349-362, rng.rs:64-72), computed on the host. */
+int ursa_gpu_betweenness(ursa_gpu_topo *t, int has_sample, double sample, int has_seed,
+                         uint64_t seed, double *out);
+/* betweenness_weighted(&Topology, &[f64], Option<f64>, Option<u64>) --
+ * algo/betweenness.rs:236-270 (ties only on exact f64 equality). */
+int ursa_gpu_betweenness_weighted(ursa_gpu_topo *t, const double *weights, uint64_t n_weights,
+                                  int has_sample, double sample, int has_seed, uint64_t seed,
+                                  double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,109 @@
+"""ctypes binding of libursa_gpu.so (the C ABI in include/ursa_gpu.h).
+
+The library is loaded from this package directory only.  If it is missing,
+importing the kernels raises: there is no CPU fallback on the product path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+GPU_SO = os.path.join(PKG, "libursa_gpu.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ETRUNC, ENODEV = range(7)
+_STATUS = {
+    EINVAL: "EINVAL",
+    ENOMEM: "ENOMEM",
+    ECUDA: "ECUDA",
+    ETIMEOUT: "ETIMEOUT",
+    ETRUNC: "ETRUNC",
+    ENODEV: "ENODEV",
+}
+
+
+class UrsaGpuError(RuntimeError):
+    """A non-OK status from the C ABI (the Rust shim would panic! here)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class PageRankParams(C.Structure):
+    """PageRankParams (ursa-core/src/algo/pagerank.rs:22-36)."""
+
+    _fields_ = [("damping", C.c_double), ("max_iter", C.c_uint32), ("tol", C.c_double)]
+
+
+class PageRankStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("last_delta", C.c_double), ("device_ms", C.c_double)]
+
+
+# Every exported symbol with its (restype, argtypes).
+P, u32, u64, i32, i64, f64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_int64, C.c_double
+SIGNATURES = {
+    "ursa_gpu_last_error": (C.c_char_p, []),
+    "ursa_gpu_version": (i32, []),
+    "ursa_gpu_launch_count": (u64, []),
+    "ursa_gpu_set_device": (i32, [i32]),
+    "ursa_gpu_topo_build": (i32, [u64, P, P, u64, C.POINTER(P)]),
+    "ursa_gpu_topo_build_device": (i32, [u64, P, P, u64, P, C.POINTER(P)]),
+    "ursa_gpu_topo_free": (None, [P]),
+    "ursa_gpu_topo_n_nodes": (u64, [P]),
+    "ursa_gpu_topo_n_edges": (u64, [P]),
+    "ursa_gpu_topo_adjacency": (i32, [P, i32, P, P, P]),
+    "ursa_gpu_topo_undirected_len": (i32, [P, C.POINTER(u64)]),
+    "ursa_gpu_topo_undirected": (i32, [P, P, P]),
+    "ursa_gpu_topo_prepare": (i32, [P, i32]),
+    "ursa_gpu_topo_device_bytes": (u64, [P]),
+    "ursa_gpu_degree": (i32, [P, i32, P]),
+    "ursa_gpu_pagerank": (i32, [P, C.POINTER(PageRankParams), P, C.POINTER(PageRankStats)]),
+    "ursa_gpu_pagerank_device": (i32, [P, C.POINTER(PageRankParams), P, P, C.POINTER(PageRankStats)]),
+    "ursa_gpu_pagerank_weighted": (
+        i32,
+        [P, P, u64, C.POINTER(PageRankParams), P, C.POINTER(PageRankStats)],
+    ),
+    "ursa_gpu_bfs_distances": (i32, [P, u32, i32, P]),
+    "ursa_gpu_shortest_path": (i32, [P, u32, u32, i32, P, u64, C.POINTER(i64)]),
+    "ursa_gpu_dijkstra_distances": (i32, [P, P, u64, u32, i32, P]),
+    "ursa_gpu_shortest_path_weighted_with_cost": (
+        i32,
+        [P, P, u64, u32, u32, i32, P, P, u64, C.POINTER(i64)],
+    ),
+    "ursa_gpu_k_hop": (i32, [P, P, u64, u32, i32, C.POINTER(P)]),
+    "ursa_gpu_pairs_len": (u64, [P]),
+    "ursa_gpu_pairs_copy": (i32, [P, P, P]),
+    "ursa_gpu_pairs_free": (None, [P]),
+    "ursa_gpu_connected_components_weak": (i32, [P, P]),
+    "ursa_gpu_triangle_count": (i32, [P, P]),
+    "ursa_gpu_clustering_coefficient": (i32, [P, P]),
+    "ursa_gpu_betweenness": (i32, [P, i32, f64, i32, u64, P]),
+    "ursa_gpu_betweenness_weighted": (i32, [P, P, u64, i32, f64, i32, u64, P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load (once) and type the in-tree libursa_gpu.so."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(GPU_SO):
+            raise ImportError(
+                f"{GPU_SO} is missing: build it with `python -m ursa_b200.build` "
+                "(the GPU kernels have no CPU fallback)"
+            )
+        L = C.CDLL(GPU_SO)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise UrsaGpuError(status, load().ursa_gpu_last_error().decode(errors="replace"))

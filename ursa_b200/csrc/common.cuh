@@ -1,0 +1,182 @@
+// common.cuh -- shared helpers for the ursa_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/ursa_gpu.h"
+
+namespace ug {
+
+// A failed CUDA call or a contract violation inside the library; caught at the
+// C-ABI boundary and turned into a status code plus a thread-local message.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define UG_CUDA(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      throw ::ug::Error(URSA_GPU_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + \
+                                          " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"); \
+    }                                                                                  \
+  } while (0)
+
+#define UG_CHECK(cond, code, msg)                  \
+  do {                                             \
+    if (!(cond)) throw ::ug::Error((code), (msg)); \
+  } while (0)
+
+// Every kernel launch in the library is followed by UG_LAUNCH_CHECK(), which
+// also counts it (ursa_gpu_launch_count), so a benchmark can report how many
+// of this library's kernels ran in a timed region.
+void count_launch();
+#define UG_LAUNCH_CHECK()          \
+  do {                             \
+    ::ug::count_launch();          \
+    UG_CUDA(cudaGetLastError());   \
+  } while (0)
+
+constexpr int kBlock = 256;
+
+inline unsigned grid_for(uint64_t n, int block = kBlock, unsigned cap = 148u * 32u) {
+  uint64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+// Stream-ordered device scratch from the device's default memory pool. The
+// pool keeps freed blocks (release threshold raised once per device), so the
+// steady state allocates nothing from the driver.
+template <class T>
+struct Scratch {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = 0;
+  Scratch() = default;
+  Scratch(size_t count, cudaStream_t st) { alloc(count, st); }
+  void alloc(size_t count, cudaStream_t st) {
+    release();
+    s = st;
+    n = count;
+    if (count) UG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  ~Scratch() { release(); }
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+  Scratch(Scratch&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+  T* get() const { return p; }
+};
+
+// Persistent device allocation (owned by a topology object).
+template <class T>
+struct DevArray {
+  T* p = nullptr;
+  size_t n = 0;
+  DevArray() = default;
+  explicit DevArray(size_t count) { alloc(count); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) UG_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevArray() { release(); }
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  DevArray(DevArray&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevArray& operator=(DevArray&& o) noexcept {
+    release();
+    p = o.p;
+    n = o.n;
+    o.p = nullptr;
+    o.n = 0;
+    return *this;
+  }
+  T* get() const { return p; }
+};
+
+// One non-blocking stream per (host thread, device): calls from different
+// host threads never serialise on a shared stream.
+cudaStream_t thread_stream(int device);
+void prepare_device(int device);
+int sm_count(int device);
+
+// Device-side timeout for bounded waits (ns since an epoch).
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded grid barrier for cooperative launches. Every block calls it the same
+// number of times. A wait longer than limit_ns sets *err and returns, so a
+// broken invariant ends the kernel with an error status instead of a hang.
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks,
+                                             int* err, uint64_t limit_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = gen;
+    unsigned g = *vgen;
+    __threadfence();
+    unsigned arrived = atomicAdd(count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      uint64_t t0 = global_ns();
+      while (*vgen == g) {
+        __nanosleep(64);
+        if (global_ns() - t0 > limit_ns) {
+          atomicExch(err, 1);
+          break;
+        }
+        if (*(volatile int*)err) break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Compensated f32 accumulator: value = hi + lo (TwoSum / Kahan-Babuska-Neumaier).
+struct F2 {
+  float hi, lo;
+};
+__device__ __forceinline__ F2 f2_zero() { return F2{0.f, 0.f}; }
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+__device__ __forceinline__ F2 f2_add(F2 a, float x) {
+  float s, e;
+  two_sum(a.hi, x, s, e);
+  return F2{s, __fadd_rn(a.lo, e)};
+}
+__device__ __forceinline__ F2 f2_combine(F2 a, F2 b) {
+  float s, e;
+  two_sum(a.hi, b.hi, s, e);
+  return F2{s, __fadd_rn(__fadd_rn(a.lo, b.lo), e)};
+}
+__device__ __forceinline__ double f2_value(F2 a) { return (double)a.hi + (double)a.lo; }
+
+}  // namespace ug

@@ -1,0 +1,35 @@
+// primitives.cuh -- device-wide scan and stable LSD radix sort used by the CSR
+// builds.  Hand-written for sm_100a; no library sort is used.
+#pragma once
+
+#include "common.cuh"
+
+namespace ug {
+
+// Exclusive prefix sum of n elements (out may alias in). If total is non-null
+// the grand total is written to *total (device pointer).
+void exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total,
+                        cudaStream_t s);
+void exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t* total,
+                        cudaStream_t s);
+
+// Stable sort of n (key, value) pairs by the low key_bits bits of the key
+// (LSD, 8-bit digits).  vals_in == nullptr means value = input position.
+// If gather_src is given, gather_out[p] = gather_src[vals_out[p]] is written
+// in the last pass (used to place the CSR targets next to their edge ids).
+// keys_out/vals_out must not alias the inputs.  n < 2^32.
+void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint64_t n, int key_bits,
+                      uint32_t* keys_out, uint32_t* vals_out, const uint32_t* gather_src,
+                      uint32_t* gather_out, cudaStream_t s);
+
+// offsets[u] = lower_bound(sorted_keys[0..m), u) for u in [0, n].
+void offsets_from_sorted(const uint32_t* sorted_keys, uint64_t m, uint64_t n, uint32_t* offsets,
+                         cudaStream_t s);
+
+inline int bits_for(uint64_t max_value) {
+  int b = 0;
+  while (b < 64 && (max_value >> b) != 0) b++;
+  return b;
+}
+
+}  // namespace ug

@@ -1,0 +1,60 @@
+// topo.cuh -- the device-resident topology behind the opaque ursa_gpu_topo.
+//
+// Mirrors ursa-core's Topology (ursa-core/src/topology.rs:251-261): the
+// out-CSR is built eagerly, the transpose and the undirected CSR lazily on
+// first use and then cached.  Device offsets are u32: ursa-core caps the edge
+// count at u32::MAX (topology.rs:61-65), so every offset fits; the host mirror
+// widens them to the reference's u64 on download.
+#pragma once
+
+#include <memory>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace ug {
+
+struct DevCsr {
+  DevArray<uint32_t> off;  // n + 1
+  DevArray<uint32_t> tgt;  // m
+  DevArray<uint32_t> eid;  // m (original edge row per slot)
+};
+
+struct PrPlan;  // PageRank work partition over the in-CSR (pagerank.cu)
+void pr_plan_free(PrPlan* p);
+uint64_t pr_plan_bytes(const PrPlan* p);
+
+struct TopoImpl {
+  int device = 0;
+  uint64_t n = 0, m = 0;
+  DevCsr out, in;
+  bool has_in = false;
+  DevArray<uint32_t> und_off, und_tgt;
+  uint64_t m_und = 0;
+  bool has_und = false;
+  DevArray<uint32_t> outdeg;  // out-degree per node (PageRank shares)
+  bool has_outdeg = false;
+  PrPlan* pr_plan = nullptr;
+  std::mutex mu;
+  ~TopoImpl() {
+    if (pr_plan) pr_plan_free(pr_plan);
+  }
+};
+
+// Stable counting-sort CSR build from device endpoint arrays (keys group,
+// other is the paired endpoint); row order is kept inside each segment.
+void build_csr(uint64_t n, const uint32_t* d_keys, const uint32_t* d_other, uint64_t m,
+               DevCsr& out, cudaStream_t s);
+// Lazily built parts; each call is a no-op once built.
+void ensure_in(TopoImpl* t, cudaStream_t s);
+void ensure_undirected(TopoImpl* t, cudaStream_t s);
+void ensure_outdeg(TopoImpl* t, cudaStream_t s);
+
+// Slot -> owning node for a CSR (binary search over offsets), n_slots = m.
+void csr_owners(const uint32_t* off, uint64_t n, uint64_t m, uint32_t* owner, cudaStream_t s);
+
+}  // namespace ug
+
+struct ursa_gpu_topo {
+  ug::TopoImpl impl;
+};
