@@ -88,22 +88,7 @@ cudaStream_t thread_stream(int device) {
   return s;
 }
 
-template <class F>
-int guard(F&& f) {
-  try {
-    f();
-    return URSA_GPU_OK;
-  } catch (const Error& e) {
-    g_last_error = e.what();
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    g_last_error = "host allocation failed";
-    return URSA_GPU_ENOMEM;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return URSA_GPU_EINVAL;
-  }
-}
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 static cudaStream_t call_stream(TopoImpl* t, void* stream) {
   cudaStream_t s = thread_stream(t->device);

@@ -79,6 +79,11 @@ struct Scratch {
   Scratch& operator=(const Scratch&) = delete;
   Scratch(Scratch&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
   T* get() const { return p; }
+  friend void swap(Scratch& a, Scratch& b) noexcept {
+    std::swap(a.p, b.p);
+    std::swap(a.n, b.n);
+    std::swap(a.s, b.s);
+  }
 };
 
 // Persistent device allocation (owned by a topology object).
@@ -112,6 +117,27 @@ struct DevArray {
   }
   T* get() const { return p; }
 };
+
+// Records the message returned by ursa_gpu_last_error() on this thread.
+void set_last_error(const std::string& msg);
+
+// Runs f() and maps exceptions to a C-ABI status code (URSA_GPU_*).
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return URSA_GPU_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return URSA_GPU_ENOMEM;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return URSA_GPU_EINVAL;
+  }
+}
 
 // One non-blocking stream per (host thread, device): calls from different
 // host threads never serialise on a shared stream.

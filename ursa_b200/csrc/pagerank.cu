@@ -10,21 +10,26 @@
 //     delta = L1(next, rank); swap; stop if delta < tol         (:85-91)
 //   returns the last `next`, no renormalisation.
 //
-// B200 design.  The in-CSR streams from HBM once per iteration; everything
-// else is per-node.  The per-edge share x[v] = rank[v]/outdeg[v] is stored as
-// f32 (4n bytes, L2-resident at R-MAT-22 scale) and gathered per in-edge; each
-// row is summed with compensated f32 (TwoSum) accumulation, then the update,
-// residual and dangling mass are computed in f64.
-//
-// Work partition (built once per topology and cached): rows with in-degree
-// <= kLong are grouped into row-aligned tiles of about kTile merge items
-// (edges + rows); rows above kLong ("hubs") are split into kChunk-edge chunks.
-// Inside a tile, the tile's shares are staged in shared memory and each
-// thread walks an equal slice of the (row-end, edge) merge path; rows that
-// cross thread slices are stitched by a block segmented scan.  A hub's chunk
-// partials are combined in chunk order by whichever chunk arrives last (an
-// arrival counter, no waiting).  One bounded grid barrier per iteration; all
-// reductions use fixed orders, so a run is bit-reproducible.
+// B200 design.
+//  * Arithmetic: the per-edge share x[v] = rank[v]/divisor[v] is stored as
+//    f32 and each row sums its shares with Kahan-compensated f32; the update,
+//    L1 residual, dangling mass and the ranks are f64.
+//  * Execution CSR (built once per topology, cached): a copy of the in-CSR
+//    with node ids relabelled by in-degree, highest first.  Rows of similar
+//    degree become contiguous, so each degree class gets a fixed group width
+//    (1..32 lanes per row, about four edges per lane) and no warp diverges on
+//    row lengths.  On R-MAT graphs in- and out-degree go together, so the
+//    smallest ids are also the most-gathered shares: the first kHot of them
+//    are copied into shared memory every iteration (about half of all gathers
+//    at R-MAT-22), taking them off L2.  Ranks return to the caller's ids at
+//    the end.
+//  * Work units: a unit is 32/G consecutive rows of a class with group width
+//    G, or a kHubChunk-edge chunk of a hub row (in-degree > kHubDeg).  Warps
+//    take units round-robin and never wait for each other inside an
+//    iteration; a hub's chunk sums are combined in chunk order by whichever
+//    chunk arrives last (an arrival counter, no waiting).
+//  * One bounded grid barrier per iteration.  Every reduction has a fixed
+//    order, so runs are bit-reproducible.
 #include <cmath>
 
 #include "primitives.cuh"
@@ -33,104 +38,137 @@
 namespace ug {
 
 namespace {
-constexpr int kTile = 2048;   // merge items per short-row tile (before the last row)
-constexpr int kLong = 1024;   // in-degree above which a row is a hub
-constexpr int kChunk = 2048;  // edges per hub chunk
-constexpr int kECap = kTile + kLong;
-constexpr int kRCap = kTile;
-constexpr uint32_t kLongFlag = 0x80000000u;
-constexpr int kPrBlock = 256;
+constexpr int kPrBlock = 1024;
 constexpr int kPrWarps = kPrBlock / 32;
+constexpr uint32_t kHubDeg = 1024;    // in-degree above which a row is chunked
+constexpr uint32_t kHubChunk = 2048;  // edges per hub chunk (64 per lane)
+constexpr int kHot = 32768;           // shares cached in shared memory (128 KB)
+constexpr int kClasses = 7;           // hub, G = 32, 16, 8, 4, 2, 1
 constexpr uint64_t kBarrierLimitNs = 5000000000ull;  // 5 s per grid barrier wait
 }  // namespace
 
+struct PrClassTable {
+  uint32_t lo[kClasses], hi[kClasses];   // row ranges (new ids)
+  uint32_t unit_begin[kClasses + 1];     // first unit of each class
+};
+
 struct PrPlan {
-  uint32_t n_work = 0, n_long = 0;
-  DevArray<uint2> work;  // short tile: {r0, r1}; hub chunk: {long index, chunk | kLongFlag}
-  DevArray<uint32_t> long_row, long_first, long_nch;
+  PrClassTable cls{};
+  uint32_t n_units = 0, n_hub = 0, n_chunks = 0;
+  DevArray<uint2> hub_unit;            // per hub chunk: {hub index, chunk}
+  DevArray<uint32_t> hub_first, hub_nch;
+  // execution CSR in relabelled ids
+  DevArray<uint32_t> old_of_new, new_of_old;
+  DevArray<uint32_t> off, src, eid;
+  DevArray<uint32_t> outdeg;  // per new id
 };
 
 void pr_plan_free(PrPlan* p) { delete p; }
 uint64_t pr_plan_bytes(const PrPlan* p) {
-  return p ? (uint64_t)p->work.n * sizeof(uint2) + 3ull * p->long_row.n * sizeof(uint32_t) : 0;
+  if (!p) return 0;
+  return (uint64_t)p->hub_unit.n * sizeof(uint2) +
+         4ull * (p->hub_first.n + p->hub_nch.n + p->old_of_new.n + p->new_of_old.n + p->off.n +
+                 p->src.n + p->eid.n + p->outdeg.n);
 }
 
 namespace {
 
 // ------------------------------------------------------------ plan kernels
-__global__ void plan_w_k(const uint32_t* __restrict__ off, uint64_t n, uint64_t* __restrict__ w) {
-  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t deg = off[u + 1] - off[u];
-    w[u] = deg > (uint32_t)kLong ? 0ull : (uint64_t)deg + 1ull;
-  }
-}
-
-__global__ void plan_flags_k(const uint32_t* __restrict__ off, uint64_t n,
-                             const uint64_t* __restrict__ W, uint32_t* __restrict__ brk,
-                             uint32_t* __restrict__ cnt, uint32_t* __restrict__ lng) {
-  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t deg = off[u + 1] - off[u];
-    bool is_long = deg > (uint32_t)kLong;
-    bool prev_long = u > 0 && (off[u] - off[u - 1]) > (uint32_t)kLong;
-    bool start = !is_long && (u == 0 || prev_long || (W[u] / kTile) != (W[u - 1] / kTile));
-    brk[u] = (start || is_long) ? 1u : 0u;
-    cnt[u] = start ? 1u : (is_long ? (deg + kChunk - 1) / kChunk : 0u);
-    lng[u] = is_long ? 1u : 0u;
-  }
-}
-
-__global__ void plan_breaks_k(uint64_t n, const uint32_t* __restrict__ brk,
-                              const uint32_t* __restrict__ bpos, uint32_t* __restrict__ B) {
+__global__ void neg_indeg_k(const uint32_t* __restrict__ off, uint64_t n, uint32_t* __restrict__ key) {
   for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
        u += (uint64_t)gridDim.x * blockDim.x)
-    if (brk[u]) B[bpos[u]] = (uint32_t)u;
+    key[u] = ~(off[u + 1] - off[u]);  // ascending ~deg == descending degree
 }
 
-__global__ void plan_fill_k(uint64_t n, const uint32_t* __restrict__ brk,
-                            const uint32_t* __restrict__ bpos, const uint32_t* __restrict__ B,
-                            const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ wpos,
-                            const uint32_t* __restrict__ lng, const uint32_t* __restrict__ lpos,
-                            uint2* __restrict__ work, uint32_t* __restrict__ long_row,
-                            uint32_t* __restrict__ long_first, uint32_t* __restrict__ long_nch) {
-  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x) {
-    if (!brk[u]) continue;
-    uint32_t wp = wpos[u];
-    if (lng[u]) {
-      uint32_t li = lpos[u], nch = cnt[u];
-      long_row[li] = (uint32_t)u;
-      long_first[li] = wp;
-      long_nch[li] = nch;
-      for (uint32_t c = 0; c < nch; c++) work[wp + c] = make_uint2(li, c | kLongFlag);
-    } else {
-      work[wp] = make_uint2((uint32_t)u, B[bpos[u] + 1]);
-    }
+__global__ void relabel_maps_k(const uint32_t* __restrict__ old_of_new, uint64_t n,
+                               const uint32_t* __restrict__ in_off,
+                               const uint32_t* __restrict__ out_off,
+                               uint32_t* __restrict__ new_of_old, uint32_t* __restrict__ deg_new,
+                               uint32_t* __restrict__ outdeg_new) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t u = old_of_new[i];
+    new_of_old[u] = (uint32_t)i;
+    deg_new[i] = in_off[u + 1] - in_off[u];
+    outdeg_new[i] = out_off[u + 1] - out_off[u];
   }
 }
 
-__global__ void set_u32_k(uint32_t* p, uint32_t v) { *p = v; }
+// Copy row old_of_new[i] of the in-CSR into new row i, relabelling sources.
+__global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n, uint64_t m,
+                               const uint32_t* __restrict__ old_of_new,
+                               const uint32_t* __restrict__ new_of_old,
+                               const uint32_t* __restrict__ in_off,
+                               const uint32_t* __restrict__ in_src,
+                               const uint32_t* __restrict__ in_eid, uint32_t* __restrict__ src_new,
+                               uint32_t* __restrict__ eid_new) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+      uint64_t mid = (lo + hi) >> 1;
+      if ((uint64_t)off_new[mid] <= k)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    uint32_t u = old_of_new[lo];
+    uint32_t slot = in_off[u] + (uint32_t)(k - off_new[lo]);
+    src_new[k] = new_of_old[in_src[slot]];
+    eid_new[k] = in_eid[slot];
+  }
+}
+
+// Class boundaries over the non-increasing degree sequence: bounds[t] =
+// number of rows with degree > thr[t].
+__global__ void class_bounds_k(const uint32_t* __restrict__ deg, uint64_t n,
+                               uint32_t* __restrict__ bounds) {
+  const uint32_t thr[kClasses - 1] = {kHubDeg, 64u, 32u, 16u, 8u, 4u};
+  for (int t = 0; t < kClasses - 1; t++) {
+    uint64_t lo = 0, hi = n;  // first index with deg <= thr
+    while (lo < hi) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (deg[mid] > thr[t])
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    bounds[t] = (uint32_t)lo;
+  }
+}
+
+__global__ void hub_nch_k(const uint32_t* __restrict__ deg, uint32_t n_hub,
+                          uint32_t* __restrict__ nch) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_hub; i += gridDim.x * blockDim.x)
+    nch[i] = (deg[i] + kHubChunk - 1) / kHubChunk;
+}
+
+__global__ void hub_units_k(const uint32_t* __restrict__ first, const uint32_t* __restrict__ nch,
+                            uint32_t n_hub, uint2* __restrict__ units) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_hub; i += gridDim.x * blockDim.x)
+    for (uint32_t c = 0; c < nch[i]; c++) units[first[i] + c] = make_uint2(i, c);
+}
 
 // ---------------------------------------------------------- iteration kernel
 struct PrArgs {
   uint64_t n;
-  const uint32_t* __restrict__ off;  // in-CSR offsets
-  const uint32_t* __restrict__ src;  // in-CSR neighbours (edge sources)
-  const uint32_t* __restrict__ outdeg;   // unweighted
-  const double* __restrict__ out_str;    // weighted (nullptr if unweighted)
-  const float* __restrict__ w_in;        // weighted: f32 weight per in-CSR slot
+  uint32_t hot;                        // shares cached in shared memory (<= kHot)
+  PrClassTable cls;
+  uint32_t n_units;
+  const uint32_t* __restrict__ off;    // execution CSR offsets (new ids)
+  const uint32_t* __restrict__ src;    // execution CSR sources (new ids)
+  const float* __restrict__ w;         // weighted: f32 weight per slot, else null
+  const uint32_t* __restrict__ outdeg;   // unweighted divisor (new ids)
+  const double* __restrict__ out_str;    // weighted divisor (new ids), else null
   double* rank[2];
   float* x[2];
-  const uint2* __restrict__ work;
-  uint32_t n_work;
-  const uint32_t* __restrict__ long_row;
-  const uint32_t* __restrict__ long_first;
-  const uint32_t* __restrict__ long_nch;
-  uint32_t n_long;
-  F2* chunk_part;         // per work item (hub chunks)
-  unsigned* long_cnt;     // per hub: chunk arrivals this iteration
-  double2* long_contrib[2];  // per hub: (|next-rank|, dangling next)
+  const uint2* __restrict__ hub_unit;
+  const uint32_t* __restrict__ hub_first;
+  const uint32_t* __restrict__ hub_nch;
+  uint32_t n_hub;
+  F2* chunk_part;            // per hub chunk
+  unsigned* hub_cnt;         // per hub: chunk arrivals this iteration
+  double2* hub_contrib[2];   // per hub: (|next-rank|, dangling next)
   double2* block_part[2];    // per block
   unsigned* bar_count;
   unsigned* bar_gen;
@@ -138,7 +176,6 @@ struct PrArgs {
   double damping;
   double tol;
   uint32_t max_iter;
-  // outputs
   uint32_t* out_iters;
   double* out_delta;
   uint32_t* out_buf;
@@ -148,43 +185,168 @@ struct Fin {
   double delta, dang;
 };
 
-__device__ __forceinline__ void finalize_row(const PrArgs& a, uint64_t u, double sum, double base,
-                                             int cur, Fin& f) {
+struct PrSmem {
+  float hot[kHot];
+  double2 dsh[kPrWarps];
+};
+
+__device__ __forceinline__ double row_divisor(const PrArgs& a, uint64_t u) {
+  return a.out_str ? a.out_str[u] : (double)a.outdeg[u];
+}
+
+__device__ __forceinline__ void finish_row(const PrArgs& a, uint64_t u, double sum, double old,
+                                           double div, double base, int cur, Fin& f) {
   // next[u] = base + d * contrib(u)   (pagerank.rs:81-83)
   double nx = __dadd_rn(base, __dmul_rn(a.damping, sum));
-  double old = a.rank[cur][u];
   f.delta += fabs(nx - old);
   a.rank[cur ^ 1][u] = nx;
-  bool dangling;
-  float share;
-  if (a.out_str) {
-    double os = a.out_str[u];
-    dangling = !(os > 0.0);
-    share = dangling ? 0.f : (float)(nx / os);
-  } else {
-    uint32_t od = a.outdeg[u];
-    dangling = od == 0;
-    share = dangling ? 0.f : (float)(nx / (double)od);
-  }
-  a.x[cur ^ 1][u] = share;
+  bool dangling = !(div > 0.0);
+  a.x[cur ^ 1][u] = dangling ? 0.f : (float)(nx / div);
   if (dangling) f.dang += nx;
 }
 
 __device__ __forceinline__ void init_row(const PrArgs& a, uint64_t u, double r0, Fin& f) {
   a.rank[0][u] = r0;
-  bool dangling;
-  float share;
-  if (a.out_str) {
-    double os = a.out_str[u];
-    dangling = !(os > 0.0);
-    share = dangling ? 0.f : (float)(r0 / os);
-  } else {
-    uint32_t od = a.outdeg[u];
-    dangling = od == 0;
-    share = dangling ? 0.f : (float)(r0 / (double)od);
-  }
-  a.x[0][u] = share;
+  double div = row_divisor(a, u);
+  bool dangling = !(div > 0.0);
+  a.x[0][u] = dangling ? 0.f : (float)(r0 / div);
   if (dangling) f.dang += r0;
+}
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  float y = __fsub_rn(v, c);
+  float t = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(t, s), y);
+  s = t;
+}
+
+// Share of source v: shared-memory copy for the hottest ids, else global.
+__device__ __forceinline__ float share(const PrArgs& a, const PrSmem& sm, const float* x,
+                                      uint32_t v) {
+  return v < a.hot ? sm.hot[v] : x[v];
+}
+
+// Sums the shares of edges [b + sub, e) with stride G; four loads in flight.
+template <int G, bool kW>
+__device__ __forceinline__ F2 row_sum(const PrArgs& a, const PrSmem& sm, const float* x, uint32_t b,
+                                      uint32_t e, int sub) {
+  float s = 0.f, c = 0.f;
+  for (uint32_t j = b + sub; j < e; j += 4 * G) {
+    uint32_t v[4];
+    float wv[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t jj = j + k * G;
+      v[k] = jj < e ? __ldcs(a.src + jj) : 0u;
+      if (kW) wv[k] = jj < e ? __ldcs(a.w + jj) : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t jj = j + k * G;
+      if (jj < e) {
+        float sv = share(a, sm, x, v[k]);
+        if (kW) sv = __fmul_rn(sv, wv[k]);
+        kahan_add(s, c, sv);
+      }
+    }
+  }
+  return F2{s, -c};
+}
+
+// Fixed-order reduction over the G lanes of a group; valid in sub == 0.
+template <int G>
+__device__ __forceinline__ F2 group_sum(F2 v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    F2 t{__shfl_down_sync(0xffffffffu, v.hi, o, G), __shfl_down_sync(0xffffffffu, v.lo, o, G)};
+    v = f2_combine(v, t);
+  }
+  return v;
+}
+
+// One unit of a row class: 32/G consecutive rows, G lanes per row.
+template <int G, bool kW>
+__device__ __forceinline__ void class_unit(const PrArgs& a, const PrSmem& sm, uint32_t lo,
+                                           uint32_t hi, uint32_t unit, int cur, double base,
+                                           Fin& f) {
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % G;
+  const uint32_t r = lo + unit * (32u / G) + (uint32_t)(lane / G);
+  const bool valid = r < hi;
+  uint32_t b = 0, e = 0;
+  double old = 0.0, div = 0.0;
+  if (valid) {
+    b = a.off[r];
+    e = a.off[r + 1];
+    if (sub == 0) {
+      old = a.rank[cur][r];
+      div = row_divisor(a, r);
+    }
+  }
+  F2 acc = row_sum<G, kW>(a, sm, a.x[cur], b, e, sub);
+  acc = group_sum<G>(acc);
+  if (valid && sub == 0) finish_row(a, r, f2_value(acc), old, div, base, cur, f);
+}
+
+template <bool kW>
+__device__ __forceinline__ void hub_unit(const PrArgs& a, const PrSmem& sm, uint32_t unit, int cur,
+                                         int parity, double base) {
+  const int lane = threadIdx.x & 31;
+  const uint2 hu = a.hub_unit[unit];
+  const uint32_t r = a.cls.lo[0] + hu.x;  // hub rows are the first rows
+  const uint32_t rb = a.off[r], re = a.off[r + 1];
+  const uint32_t eb = rb + hu.y * kHubChunk;
+  const uint32_t ee = eb + kHubChunk < re ? eb + kHubChunk : re;
+  F2 acc = row_sum<32, kW>(a, sm, a.x[cur], eb, ee, lane);
+  acc = group_sum<32>(acc);
+  if (lane == 0) {
+    const uint32_t nch = a.hub_nch[hu.x];
+    bool finish = nch == 1;
+    F2 row = acc;
+    if (!finish) {
+      a.chunk_part[unit] = acc;
+      __threadfence();
+      unsigned arrived = atomicAdd(&a.hub_cnt[hu.x], 1u);
+      if (arrived == nch - 1) {
+        __threadfence();
+        finish = true;
+        const uint32_t first = a.hub_first[hu.x];
+        row = f2_zero();
+        for (uint32_t k = 0; k < nch; k++) {
+          F2 pk;
+          pk.hi = __ldcg(&a.chunk_part[first + k].hi);
+          pk.lo = __ldcg(&a.chunk_part[first + k].lo);
+          row = f2_combine(row, pk);
+        }
+        a.hub_cnt[hu.x] = 0u;
+      }
+    }
+    if (finish) {
+      Fin g{0.0, 0.0};
+      finish_row(a, r, f2_value(row), a.rank[cur][r], row_divisor(a, r), base, cur, g);
+      a.hub_contrib[parity][hu.x] = make_double2(g.delta, g.dang);
+    }
+  }
+}
+
+template <bool kW>
+__device__ __forceinline__ void run_unit(const PrArgs& a, const PrSmem& sm, uint32_t u, int cur,
+                                         int parity, double base, Fin& f) {
+  int c = 0;
+#pragma unroll
+  for (int k = 1; k < kClasses; k++)
+    if (u >= a.cls.unit_begin[k]) c = k;
+  const uint32_t unit = u - a.cls.unit_begin[c];
+  const uint32_t lo = a.cls.lo[c], hi = a.cls.hi[c];
+  switch (c) {
+    case 0: hub_unit<kW>(a, sm, unit, cur, parity, base); break;
+    case 1: class_unit<32, kW>(a, sm, lo, hi, unit, cur, base, f); break;
+    case 2: class_unit<16, kW>(a, sm, lo, hi, unit, cur, base, f); break;
+    case 3: class_unit<8, kW>(a, sm, lo, hi, unit, cur, base, f); break;
+    case 4: class_unit<4, kW>(a, sm, lo, hi, unit, cur, base, f); break;
+    case 5: class_unit<2, kW>(a, sm, lo, hi, unit, cur, base, f); break;
+    default: class_unit<1, kW>(a, sm, lo, hi, unit, cur, base, f); break;
+  }
 }
 
 // Fixed-order block reduction of two doubles; result valid in thread 0.
@@ -207,23 +369,6 @@ __device__ __forceinline__ Fin block_sum_fin(Fin v, double2* sh) {
   return r;
 }
 
-// Fixed-order block reduction of an F2; result valid in thread 0.
-__device__ __forceinline__ F2 block_sum_f2(F2 v, F2* sh) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    F2 o2{__shfl_down_sync(0xffffffffu, v.hi, o), __shfl_down_sync(0xffffffffu, v.lo, o)};
-    v = f2_combine(v, o2);
-  }
-  __syncthreads();
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  F2 r = f2_zero();
-  if (threadIdx.x == 0)
-    for (int i = 0; i < kPrWarps; i++) r = f2_combine(r, sh[i]);
-  return r;
-}
-
 // Every block computes the same totals from the same partials in the same
 // order (warp 0, lane-strided, then a fixed shuffle tree).
 __device__ __forceinline__ Fin global_totals(const PrArgs& a, int p, double2* sh) {
@@ -234,8 +379,8 @@ __device__ __forceinline__ Fin global_totals(const PrArgs& a, int p, double2* sh
       d += v.x;
       g += v.y;
     }
-    for (uint32_t i = threadIdx.x; i < a.n_long; i += 32) {
-      double2 v = __ldcg(&a.long_contrib[p][i]);
+    for (uint32_t i = threadIdx.x; i < a.n_hub; i += 32) {
+      double2 v = __ldcg(&a.hub_contrib[p][i]);
       d += v.x;
       g += v.y;
     }
@@ -252,166 +397,46 @@ __device__ __forceinline__ Fin global_totals(const PrArgs& a, int p, double2* sh
   return r;
 }
 
-__device__ __forceinline__ void merge_path(int diag, const uint32_t* s_end, int R, int E, int& i,
-                                           int& j) {
-  int lo = diag - E > 0 ? diag - E : 0;
-  int hi = diag < R ? diag : R;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if ((int)s_end[mid] <= diag - mid - 1)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  i = lo;
-  j = diag - lo;
-}
-
-struct TileSmem {
-  float val[kECap];
-  uint32_t end[kRCap];
-  uint32_t wkey[kPrWarps];
-  F2 wval[kPrWarps];
-  F2 f2sh[kPrWarps];
-  double2 dsh[kPrWarps];
-};
-
-__device__ void short_tile(const PrArgs& a, uint32_t r0, uint32_t r1, int cur, double base,
-                           TileSmem& sm, Fin& f) {
-  const uint32_t e0 = a.off[r0];
-  const int R = (int)(r1 - r0);
-  const int E = (int)(a.off[r1] - e0);
+__device__ __forceinline__ void load_hot(const PrArgs& a, PrSmem& sm, int cur) {
   const float* __restrict__ x = a.x[cur];
-  // stage the tile's shares and row ends
-  for (int j = threadIdx.x; j < E; j += kPrBlock) {
-    uint32_t v = a.src[e0 + j];
-    float s = x[v];
-    if (a.w_in) s = __fmul_rn(s, a.w_in[e0 + j]);
-    sm.val[j] = s;
-  }
-  for (int i = threadIdx.x; i < R; i += kPrBlock) sm.end[i] = a.off[r0 + i + 1] - e0;
-  __syncthreads();
-  const int items = R + E;
-  const int ipt = (items + kPrBlock - 1) / kPrBlock;
-  int d0 = threadIdx.x * ipt;
-  if (d0 > items) d0 = items;
-  int d1 = d0 + ipt;
-  if (d1 > items) d1 = items;
-  int i, j;
-  merge_path(d0, sm.end, R, E, i, j);
-  const int first_row = i;
-  bool ended_first = false;
-  F2 first_acc = f2_zero();
-  F2 acc = f2_zero();
-  for (int d = d0; d < d1; d++) {
-    if (j < (int)sm.end[i]) {  // i < R whenever d < items
-      acc = f2_add(acc, sm.val[j]);
-      j++;
-    } else {
-      if (!ended_first) {
-        ended_first = true;
-        first_acc = acc;
-      } else {
-        finalize_row(a, (uint64_t)r0 + i, f2_value(acc), base, cur, f);
-      }
-      acc = f2_zero();
-      i++;
-    }
-  }
-  // Segmented inclusive scan of (open row, partial) over threads.
-  uint32_t key = (uint32_t)i;  // row still open at the end of the slice (R = none)
-  F2 val = acc;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t k2 = __shfl_up_sync(0xffffffffu, key, o);
-    F2 v2{__shfl_up_sync(0xffffffffu, val.hi, o), __shfl_up_sync(0xffffffffu, val.lo, o)};
-    if (lane >= o && k2 == key) val = f2_combine(v2, val);
-  }
-  if (lane == 31) {
-    sm.wkey[w] = key;
-    sm.wval[w] = val;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int ww = 1; ww < kPrWarps; ww++)
-      if (sm.wkey[ww] == sm.wkey[ww - 1]) sm.wval[ww] = f2_combine(sm.wval[ww - 1], sm.wval[ww]);
-  }
-  __syncthreads();
-  if (w > 0 && sm.wkey[w - 1] == key) val = f2_combine(sm.wval[w - 1], val);
-  // carry into this thread = inclusive value of thread t-1 (same key by construction)
-  uint32_t pk = __shfl_up_sync(0xffffffffu, key, 1);
-  F2 pv{__shfl_up_sync(0xffffffffu, val.hi, 1), __shfl_up_sync(0xffffffffu, val.lo, 1)};
-  if (lane == 0) {
-    if (w > 0) {
-      pk = sm.wkey[w - 1];
-      pv = sm.wval[w - 1];
-    } else {
-      pk = 0xffffffffu;
-    }
-  }
-  if (ended_first) {
-    F2 tot = first_acc;
-    if (threadIdx.x > 0 && pk == (uint32_t)first_row) tot = f2_combine(pv, first_acc);
-    finalize_row(a, (uint64_t)r0 + first_row, f2_value(tot), base, cur, f);
-  }
-  __syncthreads();  // smem reuse by the next tile
-}
-
-__device__ void hub_chunk(const PrArgs& a, uint32_t li, uint32_t c, uint32_t work_id, int cur,
-                          int parity, double base, TileSmem& sm) {
-  const uint32_t u = a.long_row[li];
-  const uint32_t rb = a.off[u], re = a.off[u + 1];
-  const uint32_t eb = rb + c * (uint32_t)kChunk;
-  const uint32_t ee = eb + (uint32_t)kChunk < re ? eb + (uint32_t)kChunk : re;
-  const float* __restrict__ x = a.x[cur];
-  F2 acc = f2_zero();
-  for (uint32_t e = eb + threadIdx.x; e < ee; e += kPrBlock) {
-    float s = x[a.src[e]];
-    if (a.w_in) s = __fmul_rn(s, a.w_in[e]);
-    acc = f2_add(acc, s);
-  }
-  F2 tot = block_sum_f2(acc, sm.f2sh);
-  if (threadIdx.x == 0) {
-    a.chunk_part[work_id] = tot;
-    __threadfence();
-    unsigned arrived = atomicAdd(&a.long_cnt[li], 1u);
-    if (arrived == a.long_nch[li] - 1) {
-      __threadfence();
-      uint32_t first = a.long_first[li], nch = a.long_nch[li];
-      F2 row = f2_zero();
-      for (uint32_t k = 0; k < nch; k++) {
-        F2 pk;
-        pk.hi = __ldcg(&a.chunk_part[first + k].hi);
-        pk.lo = __ldcg(&a.chunk_part[first + k].lo);
-        row = f2_combine(row, pk);
-      }
-      Fin f{0.0, 0.0};
-      finalize_row(a, u, f2_value(row), base, cur, f);
-      a.long_contrib[parity][li] = make_double2(f.delta, f.dang);
-      a.long_cnt[li] = 0u;
-    }
-  }
+  const uint32_t n4 = a.hot / 4;
+  const float4* x4 = reinterpret_cast<const float4*>(x);
+  float4* h4 = reinterpret_cast<float4*>(sm.hot);
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < n4; i += kPrBlock) h4[i] = __ldcg(x4 + i);
+  for (uint32_t i = n4 * 4 + threadIdx.x; i < a.hot; i += kPrBlock) sm.hot[i] = __ldcg(x + i);
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kPrBlock, 2) pr_persistent_k(PrArgs a) {
-  __shared__ TileSmem sm;
+template <bool kW>
+__global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PrSmem& sm = *reinterpret_cast<PrSmem*>(smem_raw);
   const double nf = (double)a.n;
+  const uint32_t gwarp = blockIdx.x * kPrWarps + (threadIdx.x >> 5);
+  const uint32_t nwarps = gridDim.x * kPrWarps;
+  const int lane = threadIdx.x & 31;
   // ---- prologue: rank_0 = 1/n, shares, dangling mass of rank_0
   {
     Fin f{0.0, 0.0};
     const double r0 = 1.0 / nf;
-    for (uint32_t wi = blockIdx.x; wi < a.n_work; wi += gridDim.x) {
-      uint2 it = a.work[wi];
-      if (it.y & kLongFlag) {
-        if ((it.y & ~kLongFlag) == 0 && threadIdx.x == 0) {
+    for (uint32_t u = gwarp; u < a.n_units; u += nwarps) {
+      int c = 0;
+#pragma unroll
+      for (int k = 1; k < kClasses; k++)
+        if (u >= a.cls.unit_begin[k]) c = k;
+      const uint32_t unit = u - a.cls.unit_begin[c];
+      if (c == 0) {
+        const uint2 hu = a.hub_unit[unit];
+        if (hu.y == 0 && lane == 0) {
           Fin g{0.0, 0.0};
-          init_row(a, a.long_row[it.x], r0, g);
-          a.long_contrib[0][it.x] = make_double2(0.0, g.dang);
+          init_row(a, a.cls.lo[0] + hu.x, r0, g);
+          a.hub_contrib[0][hu.x] = make_double2(0.0, g.dang);
         }
       } else {
-        for (uint32_t u = it.x + threadIdx.x; u < it.y; u += kPrBlock) init_row(a, u, r0, f);
+        const int G = 32 >> (c - 1);
+        const uint32_t r = a.cls.lo[c] + unit * (32u / G) + (uint32_t)(lane / G);
+        if (r < a.cls.hi[c] && lane % G == 0) init_row(a, r, r0, f);
       }
     }
     Fin b = block_sum_fin(f, sm.dsh);
@@ -429,14 +454,9 @@ __global__ void __launch_bounds__(kPrBlock, 2) pr_persistent_k(PrArgs a) {
     // base = (1-d)/n + d*dangling_mass/n   (pagerank.rs:79)
     const double base = __dadd_rn(__ddiv_rn(1.0 - a.damping, nf),
                                   __ddiv_rn(__dmul_rn(a.damping, dm), nf));
+    load_hot(a, sm, cur);
     Fin f{0.0, 0.0};
-    for (uint32_t wi = blockIdx.x; wi < a.n_work; wi += gridDim.x) {
-      uint2 w = a.work[wi];
-      if (w.y & kLongFlag)
-        hub_chunk(a, w.x, w.y & ~kLongFlag, wi, cur, parity, base, sm);
-      else
-        short_tile(a, w.x, w.y, cur, base, sm, f);
-    }
+    for (uint32_t u = gwarp; u < a.n_units; u += nwarps) run_unit<kW>(a, sm, u, cur, parity, base, f);
     Fin b = block_sum_fin(f, sm.dsh);
     if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = make_double2(b.delta, b.dang);
     grid_barrier(a.bar_count, a.bar_gen, gridDim.x, a.err, kBarrierLimitNs);
@@ -455,16 +475,18 @@ __global__ void __launch_bounds__(kPrBlock, 2) pr_persistent_k(PrArgs a) {
 }
 
 // Weighted helpers: out-strength in out-CSR slot order (pagerank.rs:148-150,
-// the same sequential order, so the f64 sums are bit-identical), and the
-// f32 weight of every in-CSR slot.
-__global__ void out_strength_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ eid,
-                               const double* __restrict__ w, uint64_t n,
-                               double* __restrict__ out_str) {
-  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x) {
+// the same sequential order, so the f64 sums are bit-identical), relabelled,
+// and the f32 weight of every execution-CSR slot.
+__global__ void out_strength_new_k(const uint32_t* __restrict__ off,
+                                   const uint32_t* __restrict__ eid, const double* __restrict__ w,
+                                   const uint32_t* __restrict__ old_of_new, uint64_t n,
+                                   double* __restrict__ out_str) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t u = old_of_new[i];
     double s = 0.0;
     for (uint32_t k = off[u]; k < off[u + 1]; k++) s += w[eid[k]];
-    out_str[u] = s;
+    out_str[i] = s;
   }
 }
 
@@ -475,128 +497,185 @@ __global__ void permute_w_f32_k(const uint32_t* __restrict__ eid, const double* 
     out[k] = (float)w[eid[k]];
 }
 
+__global__ void unpermute_k(const double* __restrict__ rank_new,
+                            const uint32_t* __restrict__ new_of_old, uint64_t n,
+                            double* __restrict__ out) {
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x)
+    out[u] = rank_new[new_of_old[u]];
+}
+
+size_t pr_smem_bytes() { return sizeof(PrSmem); }
+
 }  // namespace
 
 static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
-  const uint64_t n = t->n;
-  const uint32_t* off = t->in.off.get();
+  const uint64_t n = t->n, m = t->m;
   auto* plan = new PrPlan();
-  Scratch<uint64_t> W(n, s);
-  Scratch<uint32_t> brk(n, s), cnt(n, s), lng(n, s), bpos(n, s), wpos(n, s), lpos(n, s);
-  Scratch<uint32_t> tots(3, s);
-  plan_w_k<<<grid_for(n), kBlock, 0, s>>>(off, n, W.get());
+  // ---- relabel by in-degree, highest first (stable: ties keep id order)
+  {
+    Scratch<uint32_t> key(n, s), key_sorted(n, s);
+    neg_indeg_k<<<grid_for(n), kBlock, 0, s>>>(t->in.off.get(), n, key.get());
+    UG_LAUNCH_CHECK();
+    plan->old_of_new.alloc(n);
+    radix_sort_pairs(key.get(), nullptr, n, 32, key_sorted.get(), plan->old_of_new.get(), nullptr,
+                     nullptr, s);
+  }
+  plan->new_of_old.alloc(n);
+  plan->outdeg.alloc(n);
+  plan->off.alloc(n + 1);
+  Scratch<uint32_t> deg(n + 1, s);
+  relabel_maps_k<<<grid_for(n), kBlock, 0, s>>>(plan->old_of_new.get(), n, t->in.off.get(),
+                                                 t->out.off.get(), plan->new_of_old.get(),
+                                                 deg.get(), plan->outdeg.get());
   UG_LAUNCH_CHECK();
-  exclusive_scan_u64(W.get(), W.get(), n, nullptr, s);
-  plan_flags_k<<<grid_for(n), kBlock, 0, s>>>(off, n, W.get(), brk.get(), cnt.get(), lng.get());
-  UG_LAUNCH_CHECK();
-  exclusive_scan_u32(brk.get(), bpos.get(), n, tots.get() + 0, s);
-  exclusive_scan_u32(cnt.get(), wpos.get(), n, tots.get() + 1, s);
-  exclusive_scan_u32(lng.get(), lpos.get(), n, tots.get() + 2, s);
-  uint32_t h[3];
-  UG_CUDA(cudaMemcpyAsync(h, tots.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
-  UG_CUDA(cudaStreamSynchronize(s));
-  const uint32_t nb = h[0];
-  plan->n_work = h[1];
-  plan->n_long = h[2];
-  Scratch<uint32_t> B((size_t)nb + 1, s);
-  plan_breaks_k<<<grid_for(n), kBlock, 0, s>>>(n, brk.get(), bpos.get(), B.get());
-  UG_LAUNCH_CHECK();
-  set_u32_k<<<1, 1, 0, s>>>(B.get() + nb, (uint32_t)n);
-  UG_LAUNCH_CHECK();
-  plan->work.alloc(plan->n_work);
-  plan->long_row.alloc(plan->n_long);
-  plan->long_first.alloc(plan->n_long);
-  plan->long_nch.alloc(plan->n_long);
-  plan_fill_k<<<grid_for(n), kBlock, 0, s>>>(n, brk.get(), bpos.get(), B.get(), cnt.get(),
-                                             wpos.get(), lng.get(), lpos.get(), plan->work.get(),
-                                             plan->long_row.get(), plan->long_first.get(),
-                                             plan->long_nch.get());
-  UG_LAUNCH_CHECK();
+  UG_CUDA(cudaMemsetAsync(deg.get() + n, 0, sizeof(uint32_t), s));
+  exclusive_scan_u32(deg.get(), plan->off.get(), n + 1, nullptr, s);
+  plan->src.alloc(m ? m : 1);
+  plan->eid.alloc(m ? m : 1);
+  if (m) {
+    relabel_copy_k<<<grid_for(m), kBlock, 0, s>>>(plan->off.get(), n, m, plan->old_of_new.get(),
+                                                   plan->new_of_old.get(), t->in.off.get(),
+                                                   t->in.tgt.get(), t->in.eid.get(),
+                                                   plan->src.get(), plan->eid.get());
+    UG_LAUNCH_CHECK();
+  }
+  // ---- degree classes (rows are sorted by degree, so each is a range)
+  uint32_t bounds[kClasses - 1];
+  {
+    Scratch<uint32_t> db(kClasses - 1, s);
+    class_bounds_k<<<1, 1, 0, s>>>(deg.get(), n, db.get());
+    UG_LAUNCH_CHECK();
+    UG_CUDA(cudaMemcpyAsync(bounds, db.get(), sizeof(bounds), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  }
+  PrClassTable& c = plan->cls;
+  c.lo[0] = 0;
+  c.hi[0] = bounds[0];
+  for (int k = 1; k < kClasses; k++) {
+    c.lo[k] = bounds[k - 1];
+    c.hi[k] = k < kClasses - 1 ? bounds[k] : (uint32_t)n;
+  }
+  plan->n_hub = c.hi[0];
+  // hub chunks
+  plan->hub_nch.alloc(plan->n_hub ? plan->n_hub : 1);
+  plan->hub_first.alloc(plan->n_hub ? plan->n_hub : 1);
+  uint32_t n_chunks = 0;
+  if (plan->n_hub) {
+    Scratch<uint32_t> tot(1, s);
+    hub_nch_k<<<grid_for(plan->n_hub), kBlock, 0, s>>>(deg.get(), plan->n_hub, plan->hub_nch.get());
+    UG_LAUNCH_CHECK();
+    exclusive_scan_u32(plan->hub_nch.get(), plan->hub_first.get(), plan->n_hub, tot.get(), s);
+    UG_CUDA(cudaMemcpyAsync(&n_chunks, tot.get(), 4, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  }
+  plan->n_chunks = n_chunks;
+  plan->hub_unit.alloc(n_chunks ? n_chunks : 1);
+  if (n_chunks) {
+    hub_units_k<<<grid_for(plan->n_hub), kBlock, 0, s>>>(plan->hub_first.get(), plan->hub_nch.get(),
+                                                         plan->n_hub, plan->hub_unit.get());
+    UG_LAUNCH_CHECK();
+  }
+  c.unit_begin[0] = 0;
+  c.unit_begin[1] = n_chunks;
+  for (int k = 1; k < kClasses; k++) {
+    const uint32_t G = 32u >> (k - 1), rpu = 32u / G;
+    c.unit_begin[k + 1] = c.unit_begin[k] + (c.hi[k] - c.lo[k] + rpu - 1) / rpu;
+  }
+  plan->n_units = c.unit_begin[kClasses];
   UG_CUDA(cudaStreamSynchronize(s));
   return plan;
 }
 
 static PrPlan* ensure_pr_plan(TopoImpl* t, cudaStream_t s) {
   ensure_in(t, s);
-  ensure_outdeg(t, s);
   std::lock_guard<std::mutex> g(t->mu);
   if (!t->pr_plan) t->pr_plan = build_pr_plan(t, s);
   return t->pr_plan;
 }
 
+template <bool kW>
 static int pr_grid(int device) {
   static std::mutex mu;
   static int cached[64] = {0};
   std::lock_guard<std::mutex> g(mu);
   if (device < 0 || device >= 64) device = 0;
   if (!cached[device]) {
+    const int smem = (int)pr_smem_bytes();
+    UG_CUDA(cudaFuncSetAttribute(pr_persistent_k<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem));
     int per_sm = 0;
-    UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_persistent_k, kPrBlock, 0));
+    UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_persistent_k<kW>, kPrBlock,
+                                                          smem));
     UG_CHECK(per_sm > 0, URSA_GPU_ECUDA, "pagerank kernel cannot be resident");
     cached[device] = per_sm * sm_count(device);
   }
   return cached[device];
 }
 
-// Runs the iteration; the final ranks are left in d_out (device). Returns
-// stats. `weights` (device, by edge row) selects the weighted variant.
+// Runs the iteration; the final ranks (caller's ids) are left in d_out
+// (device).  d_weights (device, by edge row) selects the weighted variant.
 void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* d_weights,
                   double* d_out, cudaStream_t s, ursa_gpu_pagerank_stats* stats) {
-  const uint64_t n = t->n;
+  const uint64_t n = t->n, m = t->m;
   if (stats) *stats = ursa_gpu_pagerank_stats{0, 0.0, 0.0};
   if (n == 0) return;
   PrPlan* plan = ensure_pr_plan(t, s);
-  const int G = pr_grid(t->device);
+  const bool weighted = d_weights != nullptr;
+  const int G = weighted ? pr_grid<true>(t->device) : pr_grid<false>(t->device);
+  const size_t smem = pr_smem_bytes();
+  const uint32_t nh = plan->n_hub ? plan->n_hub : 1;
 
   Scratch<double> rank(2 * n, s);
-  Scratch<float> x(2 * n, s);
-  Scratch<F2> chunk_part(plan->n_work ? plan->n_work : 1, s);
-  Scratch<unsigned> long_cnt(plan->n_long ? plan->n_long : 1, s);
-  Scratch<double2> long_contrib(2 * (size_t)(plan->n_long ? plan->n_long : 1), s);
+  const uint64_t n_pad = (n + 3) & ~3ull;  // both share buffers 16-byte aligned
+  Scratch<float> x(2 * n_pad, s);
+  Scratch<F2> chunk_part(plan->n_chunks ? plan->n_chunks : 1, s);
+  Scratch<unsigned> hub_cnt(nh, s);
+  Scratch<double2> hub_contrib(2 * (size_t)nh, s);
   Scratch<double2> block_part(2 * (size_t)G, s);
-  // control block: bar_count, bar_gen, err, iters, buf | delta
-  Scratch<unsigned> ctl(8, s);
+  Scratch<unsigned> ctl(8, s);  // bar_count, bar_gen, err, iters, buf
   Scratch<double> ctl_d(1, s);
-  UG_CUDA(cudaMemsetAsync(long_cnt.get(), 0, long_cnt.n * sizeof(unsigned), s));
-  UG_CUDA(cudaMemsetAsync(long_contrib.get(), 0, long_contrib.n * sizeof(double2), s));
+  UG_CUDA(cudaMemsetAsync(hub_cnt.get(), 0, nh * sizeof(unsigned), s));
+  UG_CUDA(cudaMemsetAsync(hub_contrib.get(), 0, 2 * (size_t)nh * sizeof(double2), s));
   UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 8 * sizeof(unsigned), s));
 
   Scratch<double> out_str;
-  Scratch<float> w_in;
-  if (d_weights) {
+  Scratch<float> w_new;
+  if (weighted) {
     out_str.alloc(n, s);
-    out_strength_k<<<grid_for(n), kBlock, 0, s>>>(t->out.off.get(), t->out.eid.get(), d_weights,
-                                                   n, out_str.get());
+    out_strength_new_k<<<grid_for(n), kBlock, 0, s>>>(t->out.off.get(), t->out.eid.get(),
+                                                       d_weights, plan->old_of_new.get(), n,
+                                                       out_str.get());
     UG_LAUNCH_CHECK();
-    w_in.alloc(t->m ? t->m : 1, s);
-    if (t->m) {
-      permute_w_f32_k<<<grid_for(t->m), kBlock, 0, s>>>(t->in.eid.get(), d_weights, t->m,
-                                                         w_in.get());
+    w_new.alloc(m ? m : 1, s);
+    if (m) {
+      permute_w_f32_k<<<grid_for(m), kBlock, 0, s>>>(plan->eid.get(), d_weights, m, w_new.get());
       UG_LAUNCH_CHECK();
     }
   }
 
   PrArgs a;
   a.n = n;
-  a.off = t->in.off.get();
-  a.src = t->in.tgt.get();
-  a.outdeg = t->outdeg.get();
-  a.out_str = d_weights ? out_str.get() : nullptr;
-  a.w_in = d_weights ? w_in.get() : nullptr;
+  a.hot = (uint32_t)(n < (uint64_t)kHot ? n : (uint64_t)kHot);
+  a.cls = plan->cls;
+  a.n_units = plan->n_units;
+  a.off = plan->off.get();
+  a.src = plan->src.get();
+  a.w = weighted ? w_new.get() : nullptr;
+  a.outdeg = plan->outdeg.get();
+  a.out_str = weighted ? out_str.get() : nullptr;
   a.rank[0] = rank.get();
   a.rank[1] = rank.get() + n;
   a.x[0] = x.get();
-  a.x[1] = x.get() + n;
-  a.work = plan->work.get();
-  a.n_work = plan->n_work;
-  a.long_row = plan->long_row.get();
-  a.long_first = plan->long_first.get();
-  a.long_nch = plan->long_nch.get();
-  a.n_long = plan->n_long;
+  a.x[1] = x.get() + n_pad;
+  a.hub_unit = plan->hub_unit.get();
+  a.hub_first = plan->hub_first.get();
+  a.hub_nch = plan->hub_nch.get();
+  a.n_hub = plan->n_hub;
   a.chunk_part = chunk_part.get();
-  a.long_cnt = long_cnt.get();
-  a.long_contrib[0] = long_contrib.get();
-  a.long_contrib[1] = long_contrib.get() + (plan->n_long ? plan->n_long : 1);
+  a.hub_cnt = hub_cnt.get();
+  a.hub_contrib[0] = hub_contrib.get();
+  a.hub_contrib[1] = hub_contrib.get() + nh;
   a.block_part[0] = block_part.get();
   a.block_part[1] = block_part.get() + G;
   a.bar_count = ctl.get() + 0;
@@ -614,7 +693,8 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   UG_CUDA(cudaEventCreate(&e1));
   UG_CUDA(cudaEventRecord(e0, s));
   void* args[] = {&a};
-  UG_CUDA(cudaLaunchCooperativeKernel((void*)pr_persistent_k, dim3(G), dim3(kPrBlock), args, 0, s));
+  void* fn = weighted ? (void*)pr_persistent_k<true> : (void*)pr_persistent_k<false>;
+  UG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(kPrBlock), args, smem, s));
   count_launch();
   UG_CUDA(cudaEventRecord(e1, s));
   unsigned h[8];
@@ -628,8 +708,9 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   cudaEventDestroy(e1);
   UG_CHECK(h[2] == 0, URSA_GPU_ETIMEOUT, "pagerank: a grid barrier wait expired");
   const uint32_t buf = p.max_iter == 0 ? 0u : h[4];
-  UG_CUDA(cudaMemcpyAsync(d_out, rank.get() + (size_t)buf * n, n * sizeof(double),
-                          cudaMemcpyDeviceToDevice, s));
+  unpermute_k<<<grid_for(n), kBlock, 0, s>>>(rank.get() + (size_t)buf * n, plan->new_of_old.get(),
+                                             n, d_out);
+  UG_LAUNCH_CHECK();
   if (stats) {
     stats->iterations = h[3];
     stats->last_delta = hd;
