@@ -44,6 +44,8 @@ constexpr uint32_t kHubDeg = 1024;    // in-degree above which a row is chunked
 constexpr uint32_t kHubChunk = 2048;  // edges per hub chunk (64 per lane)
 constexpr int kHot = 32768;           // shares cached in shared memory (128 KB)
 constexpr int kClasses = 7;           // hub, G = 32, 16, 8, 4, 2, 1
+constexpr int kBatchWide = 8;         // loads in flight per lane, 32-lane rows
+constexpr int kBatchHub = 16;         // loads in flight per lane, hub chunks
 constexpr uint64_t kBarrierLimitNs = 5000000000ull;  // 5 s per grid barrier wait
 }  // namespace
 
@@ -226,29 +228,32 @@ __device__ __forceinline__ float share(const PrArgs& a, const PrSmem& sm, const 
   return v < a.hot ? sm.hot[v] : x[v];
 }
 
-// Sums the shares of edges [b + sub, e) with stride G; four loads in flight.
-template <int G, bool kW>
+// Sums the shares of edges [b + sub, e) with stride G; B source loads (and
+// then B gathers) in flight per lane.
+template <int G, bool kW, int B>
 __device__ __forceinline__ F2 row_sum(const PrArgs& a, const PrSmem& sm, const float* x, uint32_t b,
                                       uint32_t e, int sub) {
   float s = 0.f, c = 0.f;
-  for (uint32_t j = b + sub; j < e; j += 4 * G) {
-    uint32_t v[4];
-    float wv[4];
+  for (uint32_t j = b + sub; j < e; j += B * G) {
+    uint32_t v[B];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < B; k++) {
       uint32_t jj = j + k * G;
       v[k] = jj < e ? __ldcs(a.src + jj) : 0u;
-      if (kW) wv[k] = jj < e ? __ldcs(a.w + jj) : 0.f;
     }
+    float sv[B];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < B; k++) {
       uint32_t jj = j + k * G;
+      sv[k] = 0.f;
       if (jj < e) {
-        float sv = share(a, sm, x, v[k]);
-        if (kW) sv = __fmul_rn(sv, wv[k]);
-        kahan_add(s, c, sv);
+        sv[k] = share(a, sm, x, v[k]);
+        if (kW) sv[k] = __fmul_rn(sv[k], __ldcs(a.w + jj));
       }
     }
+#pragma unroll
+    for (int k = 0; k < B; k++)
+      if (j + k * G < e) kahan_add(s, c, sv[k]);
   }
   return F2{s, -c};
 }
@@ -283,7 +288,7 @@ __device__ __forceinline__ void class_unit(const PrArgs& a, const PrSmem& sm, ui
       div = row_divisor(a, r);
     }
   }
-  F2 acc = row_sum<G, kW>(a, sm, a.x[cur], b, e, sub);
+  F2 acc = row_sum<G, kW, (G >= 32 ? kBatchWide : 4)>(a, sm, a.x[cur], b, e, sub);
   acc = group_sum<G>(acc);
   if (valid && sub == 0) finish_row(a, r, f2_value(acc), old, div, base, cur, f);
 }
@@ -297,7 +302,7 @@ __device__ __forceinline__ void hub_unit(const PrArgs& a, const PrSmem& sm, uint
   const uint32_t rb = a.off[r], re = a.off[r + 1];
   const uint32_t eb = rb + hu.y * kHubChunk;
   const uint32_t ee = eb + kHubChunk < re ? eb + kHubChunk : re;
-  F2 acc = row_sum<32, kW>(a, sm, a.x[cur], eb, ee, lane);
+  F2 acc = row_sum<32, kW, kBatchHub>(a, sm, a.x[cur], eb, ee, lane);
   acc = group_sum<32>(acc);
   if (lane == 0) {
     const uint32_t nch = a.hub_nch[hu.x];
