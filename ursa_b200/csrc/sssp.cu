@@ -75,6 +75,34 @@ __global__ void unqueue_k(const uint32_t* __restrict__ N, uint32_t cnt, uint32_t
     inq[N[i]] = 0u;
 }
 
+// Hop levels over tight edges (fl(dist[u] + w) == dist[v]) from the source;
+// used to walk paths when zero-weight edges create equal-distance ties.
+__global__ void tight_level_k(DirView d, const double* __restrict__ w0, const double* __restrict__ w1,
+                              const uint32_t* __restrict__ F, uint64_t f,
+                              const uint64_t* __restrict__ pos, uint64_t T,
+                              const unsigned long long* __restrict__ dist, int32_t* level,
+                              int32_t lvl, uint32_t* __restrict__ N, uint32_t* __restrict__ cnt) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t span = ((T + stride - 1) / stride) * stride;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < span; e += stride) {
+    bool take = false;
+    uint32_t v = 0;
+    if (e < T) {
+      uint64_t i = owner_in_pos(pos, f, e);
+      uint32_t u = F[i];
+      uint32_t slot;
+      bool second;
+      v = dv_nbr(d, u, (uint32_t)(e - pos[i]), &slot, &second);
+      double w = second ? w1[slot] : w0[slot];
+      double nd = __dadd_rn(__longlong_as_double((long long)dist[u]), w);
+      if ((unsigned long long)__double_as_longlong(nd) == dist[v] && dist[v] != kInfBits &&
+          level[v] < 0)
+        take = atomicCAS(&level[v], -1, lvl + 1) == -1;
+    }
+    append_w(N, cnt, take, v);
+  }
+}
+
 __global__ void fill_u64_k(unsigned long long* p, uint64_t n, unsigned long long v) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
@@ -89,10 +117,12 @@ __global__ void seed_k(unsigned long long* dist, uint32_t* F, uint32_t source) {
 // One block walks the path back from the target: at node v it scans the
 // reverse adjacency for tight predecessors and keeps the smallest
 // (dist, id), restricted to (dist[u], u) < (dist[v], v) so a zero-weight
-// cycle cannot loop.
+// cycle cannot loop -- or, when level is given, to predecessors one tight
+// hop closer to the source.
 __global__ void weighted_backtrack_k(DirView rev, const double* __restrict__ rw0,
                                      const double* __restrict__ rw1,
-                                     const unsigned long long* __restrict__ dist, uint32_t source,
+                                     const unsigned long long* __restrict__ dist,
+                                     const int32_t* __restrict__ level, uint32_t source,
                                      uint32_t target, uint64_t cap, uint32_t* __restrict__ path,
                                      unsigned long long* __restrict__ out_len) {
   __shared__ unsigned long long best_d[kBlock / 32];
@@ -126,7 +156,8 @@ __global__ void weighted_backtrack_k(DirView rev, const double* __restrict__ rw0
       double w = second ? rw1[slot] : rw0[slot];
       double nd = __dadd_rn(__longlong_as_double((long long)du), w);
       if ((unsigned long long)__double_as_longlong(nd) != dv || !(nd == dvd)) continue;
-      bool before = du < dv || (du == dv && u < v);
+      bool before = level ? (level[u] >= 0 && level[u] + 1 == level[v])
+                          : (du < dv || (du == dv && u < v));
       if (!before) continue;
       if (du < bd || (du == bd && u < bu)) {
         bd = du;
@@ -242,12 +273,41 @@ int64_t weighted_path_run(TopoImpl* t, const double* d_weights, uint32_t source,
   gather_dir_weights(t, rv, d_weights, rw, s);
   Scratch<uint32_t> dpath(n, s);
   Scratch<unsigned long long> dlen(1, s);
-  weighted_backtrack_k<<<1, kBlock, 0, s>>>(rv, rw.w0.get(), rw.w1.get(), dist.get(), source,
-                                            target, n, dpath.get(), dlen.get());
+  weighted_backtrack_k<<<1, kBlock, 0, s>>>(rv, rw.w0.get(), rw.w1.get(), dist.get(), nullptr,
+                                            source, target, n, dpath.get(), dlen.get());
   UG_LAUNCH_CHECK();
   unsigned long long len = 0;
   UG_CUDA(cudaMemcpyAsync(&len, dlen.get(), 8, cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaStreamSynchronize(s));
+  if (len == 0) {
+    // Zero-weight ties: walk back along hop levels of the tight-edge graph.
+    Scratch<int32_t> level(n, s);
+    UG_CUDA(cudaMemsetAsync(level.get(), 0xFF, n * sizeof(int32_t), s));
+    FrontierBufs b;
+    b.alloc(n, s);
+    UG_CUDA(cudaMemsetAsync(level.get() + source, 0, sizeof(int32_t), s));
+    UG_CUDA(cudaMemcpyAsync(b.F.get(), &source, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    uint32_t f = 1;
+    int32_t lvl = 0;
+    while (f > 0) {
+      uint64_t T = frontier_scan(d, b.F.get(), f, b.pos.get(), s);
+      if (T == 0) break;
+      UG_CUDA(cudaMemsetAsync(b.count.get(), 0, sizeof(uint32_t), s));
+      tight_level_k<<<grid_for(T, kBlock, 148u * 64u), kBlock, 0, s>>>(
+          d, w.w0.get(), w.w1.get(), b.F.get(), f, b.pos.get(), T, dist.get(), level.get(), lvl,
+          b.N.get(), b.count.get());
+      UG_LAUNCH_CHECK();
+      uint32_t next = read_u32(b.count.get(), s);
+      swap(b.F, b.N);
+      f = next;
+      lvl++;
+    }
+    weighted_backtrack_k<<<1, kBlock, 0, s>>>(rv, rw.w0.get(), rw.w1.get(), dist.get(), level.get(),
+                                              source, target, n, dpath.get(), dlen.get());
+    UG_LAUNCH_CHECK();
+    UG_CUDA(cudaMemcpyAsync(&len, dlen.get(), 8, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  }
   UG_CHECK(len > 0, URSA_GPU_EINVAL, "weighted path walk found no predecessor");
   if (len > cap) return -(int64_t)len - 2;
   // reverse into forward order on the host copy
