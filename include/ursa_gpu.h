@@ -177,6 +177,24 @@ void ursa_gpu_pairs_free(ursa_gpu_pairs *p);
  * representative, and the partition is identical). */
 int ursa_gpu_connected_components_weak(ursa_gpu_topo *t, uint32_t *out);
 
+/* Allocation-free form of ursa_gpu_connected_components_weak.  It has no
+ * counterpart in the reference; it exists for callers that must not have the
+ * library allocate device memory while they run a query -- a serving loop
+ * whose free HBM is already promised to resident graphs, or a host runtime
+ * that owns all device memory through its own pool.  The call allocates
+ * nothing: the labels go to the caller's device array d_labels (n u32, same
+ * minimum-member labels as the allocating form) and the union-find scratch
+ * is a fixed array inside the library, 16 MiB per GPU, held by every GPU
+ * that loads the library until the process exits.
+ *  - Graphs above 4,194,304 nodes are rejected with URSA_GPU_EINVAL.
+ *  - The first call on a device looks up that array's device address; make
+ *    that first call before any stream capture.
+ *  - All calls on one GPU share the array: calls that overlap on the GPU
+ *    (other threads, other streams) race and must be serialised by the caller.
+ *  - stream: a cudaStream_t, or NULL for this thread's stream; the call
+ *    returns after the kernels finish. */
+int ursa_gpu_connected_components_weak_noalloc(ursa_gpu_topo *t, uint32_t *d_labels, void *stream);
+
 /* triangle_count(&Topology) -> Vec<u32> -- algo/triangle.rs:40-62: triangles
  * through each node of the undirected simple view. */
 int ursa_gpu_triangle_count(ursa_gpu_topo *t, uint32_t *out);

@@ -77,6 +77,7 @@ SIGNATURES = {
     "ursa_gpu_pairs_copy": (i32, [P, P, P]),
     "ursa_gpu_pairs_free": (None, [P]),
     "ursa_gpu_connected_components_weak": (i32, [P, P]),
+    "ursa_gpu_connected_components_weak_noalloc": (i32, [P, P, P]),
     "ursa_gpu_triangle_count": (i32, [P, P]),
     "ursa_gpu_clustering_coefficient": (i32, [P, P]),
     "ursa_gpu_betweenness": (i32, [P, i32, f64, i32, u64, P]),

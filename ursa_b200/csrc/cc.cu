@@ -104,6 +104,23 @@ void cc_weak_run(TopoImpl* t, uint32_t* d_out, cudaStream_t s) {
   UG_LAUNCH_CHECK();
 }
 
+// The same kernels with a caller-supplied parent array (n u32, overwritten):
+// used by the allocation-free entry point.
+void cc_weak_with_parent(TopoImpl* t, uint32_t* parent, uint32_t* d_out, cudaStream_t s) {
+  const uint64_t n = t->n, m = t->m;
+  if (n == 0) return;
+  iota_k<<<grid_for(n), kBlock, 0, s>>>(parent, n);
+  UG_LAUNCH_CHECK();
+  if (m) {
+    union_edges_k<<<grid_for(m, kBlock, 148u * 64u), kBlock, 0, s>>>(t->out.off.get(),
+                                                                      t->out.tgt.get(), n, m,
+                                                                      parent);
+    UG_LAUNCH_CHECK();
+  }
+  flatten_k<<<grid_for(n), kBlock, 0, s>>>(parent, n, d_out);
+  UG_LAUNCH_CHECK();
+}
+
 }  // namespace ug
 
 using namespace ug;
