@@ -1,0 +1,411 @@
+// bc.cu -- Brandes betweenness (ursa-core/src/algo/betweenness.rs, rng.rs).
+//
+// Sources: all nodes, or the reference's seeded sample -- the first
+// ceil(frac * n) entries of a SplitMix64 Fisher-Yates shuffle
+// (betweenness.rs:349-362, rng.rs:12-72) -- computed on the host, so the
+// device uses exactly the reference's source set for a given seed.
+//
+// Per source, on the device:
+//  * unweighted (brandes_from, :185-230): level-synchronous BFS over the
+//    out-CSR; sigma[w] += sigma[v] for every CSR slot v->w with
+//    dist[w] = dist[v] + 1 (parallel edges count, as in the reference), as f64
+//    atomics -- shortest-path counts are integers, exact below 2^53, so the
+//    order of those additions does not matter;
+//  * weighted (brandes_from_weighted, :278-339): Dijkstra-equivalent f64
+//    distances (frontier Bellman-Ford), then the tight-edge DAG
+//    (fl(dist[u] + w) == dist[v], exact equality as the reference's tie rule)
+//    is walked in Kahn order to accumulate sigma;
+//  * reverse accumulation (reverse_accumulate, :81-98): levels in reverse,
+//    one warp per node sums sigma[v] * ((1 + delta[w]) / sigma[w]) over its
+//    DAG successors with a fixed-order reduction, then bc += delta (source
+//    excluded).
+// Sources go in 64-source chunks whose partial vectors are added in chunk
+// order, and sampled results are scaled by n / k (accumulate_sources,
+// :45-70; :171-176).  The dependency sums run in a different order than the
+// reference's predecessor lists, so results agree to f64 rounding.
+#include <cmath>
+#include <vector>
+
+#include "frontier.cuh"
+
+namespace ug {
+
+void sssp_run(const DirView& d, const double* w0, const double* w1, uint64_t n, uint32_t source,
+              unsigned long long* dist, cudaStream_t s);
+
+namespace {
+
+constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;
+constexpr uint32_t kSrcChunk = 64;  // betweenness.rs:51
+
+// ---------------------------------------------------------------- rng.rs
+constexpr uint64_t kDefaultSeed = 0x5EED5EED5EED5EEDull;  // rng.rs:9
+
+uint64_t splitmix_next(uint64_t& state) {
+  state += 0x9E3779B97F4A7C15ull;
+  uint64_t z = state;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// sample_sources (betweenness.rs:349-362) with shuffled_order (rng.rs:64-72).
+std::vector<uint32_t> sample_sources(uint64_t n, bool has_sample, double frac, bool has_seed,
+                                     uint64_t seed) {
+  std::vector<uint32_t> out;
+  if (!has_sample) {
+    out.resize(n);
+    for (uint64_t i = 0; i < n; i++) out[i] = (uint32_t)i;
+    return out;
+  }
+  double f = frac;
+  if (f < 0.0) f = 0.0;
+  if (f > 1.0) f = 1.0;
+  double kf = std::ceil((double)n * f);
+  uint64_t k = (std::isnan(kf) || kf <= 0.0) ? 0 : (kf >= 1.8446744073709552e19 ? UINT64_MAX : (uint64_t)kf);
+  if (k < 1) k = 1;
+  if (k > n) k = n;
+  if (k == 0) return out;
+  std::vector<uint32_t> order(n);
+  for (uint64_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+  uint64_t st = (has_seed ? seed : kDefaultSeed) ^ 0xD1B54A32D192ED03ull;
+  for (uint64_t i = n; i-- > 1;) {
+    uint64_t j = splitmix_next(st) % (i + 1);
+    std::swap(order[i], order[j]);
+  }
+  out.assign(order.begin(), order.begin() + k);
+  return out;
+}
+
+// ------------------------------------------------------------ kernels
+__device__ __forceinline__ void append_bc(uint32_t* Q, uint32_t* cnt, bool take, uint32_t v) {
+  uint32_t mask = __ballot_sync(0xffffffffu, take);
+  if (!take) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  Q[base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+__global__ void bfs_discover_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                               const uint32_t* __restrict__ F, uint64_t f,
+                               const uint64_t* __restrict__ pos, uint64_t T, int32_t* dist,
+                               int32_t level, uint32_t* __restrict__ N, uint32_t* __restrict__ cnt) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t span = ((T + stride - 1) / stride) * stride;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < span; e += stride) {
+    bool take = false;
+    uint32_t v = 0;
+    if (e < T) {
+      uint64_t i = owner_in_pos(pos, f, e);
+      v = tgt[off[F[i]] + (uint32_t)(e - pos[i])];
+      if (dist[v] < 0) take = atomicCAS(&dist[v], -1, level + 1) == -1;
+    }
+    append_bc(N, cnt, take, v);
+  }
+}
+
+__global__ void bfs_sigma_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                            const uint32_t* __restrict__ F, uint64_t f,
+                            const uint64_t* __restrict__ pos, uint64_t T,
+                            const int32_t* __restrict__ dist, int32_t level, double* sigma) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < T;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t i = owner_in_pos(pos, f, e);
+    uint32_t u = F[i];
+    uint32_t v = tgt[off[u] + (uint32_t)(e - pos[i])];
+    if (dist[v] == level + 1) atomicAdd(&sigma[v], sigma[u]);
+  }
+}
+
+__device__ __forceinline__ bool tight(const unsigned long long* __restrict__ dist, uint32_t u,
+                                      uint32_t v, double w) {
+  unsigned long long du = dist[u], dv = dist[v];
+  if (du == kInfBits || u == v) return false;
+  double nd = __dadd_rn(__longlong_as_double((long long)du), w);
+  if ((unsigned long long)__double_as_longlong(nd) != dv) return false;
+  return du < dv || (du == dv && u < v);  // zero weights: keep the DAG acyclic
+}
+
+// tight in-slot counts over every out-slot (owner by binary search)
+__global__ void tight_indeg_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                              const double* __restrict__ w, uint64_t n, uint64_t m,
+                              const unsigned long long* __restrict__ dist,
+                              uint32_t* __restrict__ indeg) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+      uint64_t mid = (lo + hi) >> 1;
+      if ((uint64_t)off[mid] <= k)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    uint32_t u = (uint32_t)lo, v = tgt[k];
+    if (tight(dist, u, v, w[k])) atomicAdd(&indeg[v], 1u);
+  }
+}
+
+__global__ void kahn_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                       const double* __restrict__ w, const uint32_t* __restrict__ F, uint64_t f,
+                       const uint64_t* __restrict__ pos, uint64_t T,
+                       const unsigned long long* __restrict__ dist, uint32_t* indeg, double* sigma,
+                       uint32_t* __restrict__ N, uint32_t* __restrict__ cnt) {
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t span = ((T + stride - 1) / stride) * stride;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < span; e += stride) {
+    bool take = false;
+    uint32_t v = 0;
+    if (e < T) {
+      uint64_t i = owner_in_pos(pos, f, e);
+      uint32_t u = F[i];
+      uint32_t k = off[u] + (uint32_t)(e - pos[i]);
+      v = tgt[k];
+      if (tight(dist, u, v, w[k])) {
+        atomicAdd(&sigma[v], sigma[u]);
+        take = atomicSub(&indeg[v], 1u) == 1u;
+      }
+    }
+    append_bc(N, cnt, take, v);
+  }
+}
+
+// One warp per node of the level: delta[v] = sum over DAG successors of
+// sigma[v] * ((1 + delta[w]) / sigma[w]); bc[v] += delta[v] unless v == s.
+template <bool kWeighted>
+__global__ void dependency_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                             const double* __restrict__ w, const uint32_t* __restrict__ L,
+                             uint64_t cnt, const int32_t* __restrict__ hop,
+                             const unsigned long long* __restrict__ dist,
+                             const double* __restrict__ sigma, double* delta, double* bc,
+                             uint32_t source) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i = warp; i < cnt; i += nwarps) {
+    const uint32_t v = L[i];
+    const double sv = sigma[v];
+    double acc = 0.0;
+    for (uint32_t k = off[v] + lane; k < off[v + 1]; k += 32) {
+      const uint32_t x = tgt[k];
+      bool succ = kWeighted ? tight(dist, v, x, w[k]) : (hop[x] == hop[v] + 1);
+      if (succ) acc += __dmul_rn(sv, __ddiv_rn(__dadd_rn(1.0, delta[x]), sigma[x]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      delta[v] = acc;
+      if (v != source) bc[v] += acc;
+    }
+  }
+}
+
+__global__ void add_into_k(double* __restrict__ dst, const double* __restrict__ src, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = __dadd_rn(dst[i], src[i]);
+}
+
+__global__ void scale_k(double* __restrict__ x, uint64_t n, double s) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    x[i] = __dmul_rn(x[i], s);
+}
+
+__global__ void seed_source_k(int32_t* hop, double* sigma, uint32_t* L, uint32_t s) {
+  if (hop) hop[s] = 0;
+  sigma[s] = 1.0;
+  L[0] = s;
+}
+
+__global__ void fdeg_out_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ F,
+                           uint64_t f, uint64_t* __restrict__ pos) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= f;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    pos[i] = i < f ? (uint64_t)(off[F[i] + 1] - off[F[i]]) : 0ull;
+}
+
+}  // namespace
+
+struct BcState {
+  Scratch<int32_t> hop;                 // unweighted BFS level (-1 = unreached)
+  Scratch<unsigned long long> dist;     // weighted distance bits
+  Scratch<uint32_t> indeg;              // weighted: tight in-slots left
+  Scratch<double> sigma, delta;
+  Scratch<uint32_t> L;                  // nodes in discovery order, by level
+  Scratch<uint64_t> pos;
+  Scratch<uint32_t> cnt;
+};
+
+static uint64_t out_scan(const uint32_t* off, const uint32_t* F, uint64_t f, uint64_t* pos,
+                         cudaStream_t s) {
+  fdeg_out_k<<<grid_for(f + 1), kBlock, 0, s>>>(off, F, f, pos);
+  UG_LAUNCH_CHECK();
+  exclusive_scan_u64(pos, pos, f + 1, nullptr, s);
+  uint64_t total = 0;
+  UG_CUDA(cudaMemcpyAsync(&total, pos + f, 8, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  return total;
+}
+
+// One source's dependencies added into acc.
+static void brandes_source(TopoImpl* t, const double* w_out, uint32_t src, BcState& st,
+                           double* acc, cudaStream_t s) {
+  const uint64_t n = t->n, m = t->m;
+  const uint32_t* off = t->out.off.get();
+  const uint32_t* tgt = t->out.tgt.get();
+  const bool weighted = w_out != nullptr;
+  UG_CUDA(cudaMemsetAsync(st.sigma.get(), 0, n * 8, s));
+  UG_CUDA(cudaMemsetAsync(st.delta.get(), 0, n * 8, s));
+  if (weighted) {
+    DirView dv{};
+    dv.off0 = off;
+    dv.tgt0 = tgt;
+    dv.eid0 = t->out.eid.get();
+    sssp_run(dv, w_out, nullptr, n, src, st.dist.get(), s);
+    UG_CUDA(cudaMemsetAsync(st.indeg.get(), 0, n * 4, s));
+    if (m) {
+      tight_indeg_k<<<grid_for(m, kBlock, 148u * 64u), kBlock, 0, s>>>(off, tgt, w_out, n, m,
+                                                                        st.dist.get(),
+                                                                        st.indeg.get());
+      UG_LAUNCH_CHECK();
+    }
+  } else {
+    UG_CUDA(cudaMemsetAsync(st.hop.get(), 0xFF, n * 4, s));
+  }
+  seed_source_k<<<1, 1, 0, s>>>(weighted ? nullptr : st.hop.get(), st.sigma.get(), st.L.get(), src);
+  UG_LAUNCH_CHECK();
+  std::vector<uint64_t> lev = {0, 1};  // level l = L[lev[l] .. lev[l+1])
+  int32_t level = 0;
+  while (true) {
+    const uint64_t lo = lev[lev.size() - 2], hi = lev.back();
+    const uint64_t f = hi - lo;
+    if (f == 0) break;
+    const uint32_t* F = st.L.get() + lo;
+    uint64_t T = out_scan(off, F, f, st.pos.get(), s);
+    if (T == 0) {
+      lev.push_back(hi);
+      break;
+    }
+    UG_CUDA(cudaMemsetAsync(st.cnt.get(), 0, 4, s));
+    unsigned g = grid_for(T, kBlock, 148u * 64u);
+    if (weighted) {
+      kahn_k<<<g, kBlock, 0, s>>>(off, tgt, w_out, F, f, st.pos.get(), T, st.dist.get(),
+                                  st.indeg.get(), st.sigma.get(), st.L.get() + hi, st.cnt.get());
+      UG_LAUNCH_CHECK();
+    } else {
+      bfs_discover_k<<<g, kBlock, 0, s>>>(off, tgt, F, f, st.pos.get(), T, st.hop.get(), level,
+                                          st.L.get() + hi, st.cnt.get());
+      UG_LAUNCH_CHECK();
+      bfs_sigma_k<<<g, kBlock, 0, s>>>(off, tgt, F, f, st.pos.get(), T, st.hop.get(), level,
+                                       st.sigma.get());
+      UG_LAUNCH_CHECK();
+    }
+    uint32_t next = read_u32(st.cnt.get(), s);
+    lev.push_back(hi + next);
+    level++;
+  }
+  // reverse accumulation, deepest level first
+  for (size_t l = lev.size() - 1; l-- > 0;) {
+    const uint64_t lo = lev[l], hi = lev[l + 1];
+    if (hi <= lo) continue;
+    const uint64_t cnt = hi - lo;
+    unsigned g = grid_for(cnt * 32, kBlock, 148u * 64u);
+    if (weighted)
+      dependency_k<true><<<g, kBlock, 0, s>>>(off, tgt, w_out, st.L.get() + lo, cnt, nullptr,
+                                              st.dist.get(), st.sigma.get(), st.delta.get(), acc,
+                                              src);
+    else
+      dependency_k<false><<<g, kBlock, 0, s>>>(off, tgt, nullptr, st.L.get() + lo, cnt,
+                                               st.hop.get(), nullptr, st.sigma.get(),
+                                               st.delta.get(), acc, src);
+    UG_LAUNCH_CHECK();
+  }
+}
+
+void betweenness_run(TopoImpl* t, const double* d_weights, bool has_sample, double sample,
+                     bool has_seed, uint64_t seed, double* d_out, cudaStream_t s) {
+  const uint64_t n = t->n, m = t->m;
+  if (n == 0) return;
+  std::vector<uint32_t> sources = sample_sources(n, has_sample, sample, has_seed, seed);
+  UG_CUDA(cudaMemsetAsync(d_out, 0, n * 8, s));
+  if (sources.empty()) return;
+  BcState st;
+  st.sigma.alloc(n, s);
+  st.delta.alloc(n, s);
+  st.L.alloc(n, s);
+  st.pos.alloc(n + 1, s);
+  st.cnt.alloc(1, s);
+  Scratch<double> w_out;
+  if (d_weights) {
+    st.dist.alloc(n, s);
+    st.indeg.alloc(n, s);
+    w_out.alloc(m ? m : 1, s);
+    DirView dv{};
+    dv.off0 = t->out.off.get();
+    dv.tgt0 = t->out.tgt.get();
+    dv.eid0 = t->out.eid.get();
+    DirWeights dw;
+    gather_dir_weights(t, dv, d_weights, dw, s);
+    swap(w_out, dw.w0);
+  } else {
+    st.hop.alloc(n, s);
+  }
+  Scratch<double> acc(n, s);
+  for (size_t c0 = 0; c0 < sources.size(); c0 += kSrcChunk) {
+    UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * 8, s));
+    size_t c1 = c0 + kSrcChunk < sources.size() ? c0 + kSrcChunk : sources.size();
+    for (size_t i = c0; i < c1; i++)
+      brandes_source(t, d_weights ? w_out.get() : nullptr, sources[i], st, acc.get(), s);
+    add_into_k<<<grid_for(n), kBlock, 0, s>>>(d_out, acc.get(), n);
+    UG_LAUNCH_CHECK();
+  }
+  if (has_sample) {
+    scale_k<<<grid_for(n), kBlock, 0, s>>>(d_out, n, (double)n / (double)sources.size());
+    UG_LAUNCH_CHECK();
+  }
+}
+
+}  // namespace ug
+
+using namespace ug;
+
+extern "C" {
+
+int ursa_gpu_betweenness(ursa_gpu_topo* t, int has_sample, double sample, int has_seed,
+                         uint64_t seed, double* out) {
+  return guard([&] {
+    UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
+    TopoImpl* ti = &t->impl;
+    if (ti->n == 0) return;  // betweenness.rs:155-157
+    UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
+    cudaStream_t s = thread_stream(ti->device);
+    Scratch<double> d(ti->n, s);
+    betweenness_run(ti, nullptr, has_sample != 0, sample, has_seed != 0, seed, d.get(), s);
+    UG_CUDA(cudaMemcpyAsync(out, d.get(), ti->n * 8, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int ursa_gpu_betweenness_weighted(ursa_gpu_topo* t, const double* weights, uint64_t n_weights,
+                                  int has_sample, double sample, int has_seed, uint64_t seed,
+                                  double* out) {
+  return guard([&] {
+    UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
+    TopoImpl* ti = &t->impl;
+    UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
+    if (ti->n == 0) return;  // betweenness.rs:248-250
+    UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
+    cudaStream_t s = thread_stream(ti->device);
+    Scratch<double> dw(ti->m ? ti->m : 1, s), d(ti->n, s);
+    if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
+    betweenness_run(ti, dw.get(), has_sample != 0, sample, has_seed != 0, seed, d.get(), s);
+    UG_CUDA(cudaMemcpyAsync(out, d.get(), ti->n * 8, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"
