@@ -45,9 +45,9 @@ DAMPING, TOL, MAX_ITER = 0.85, 1e-6, 100
 WORKLOAD = "rmat22_pagerank"
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one pr_persistent_k launch on
-# this workload, from the ncu capture summarised in
-# profiles/pagerank_rmat22.md (None until captured).
-NCU_TRAFFIC = None  # {"bytes_per_launch": B, "iterations": I}
+# this workload (prologue + 5 fixed iterations), from the ncu capture
+# summarised in profiles/pagerank_rmat22.md.
+NCU_TRAFFIC = {"bytes_per_launch": 1_685_397_000 + 261_330_176, "iterations": 5}
 
 
 def env_int(name, default):
@@ -331,8 +331,10 @@ def main():
         peak, peak_kind = load_peaks()
         traffic = None
         if NCU_TRAFFIC:
-            per_iter = NCU_TRAFFIC["bytes_per_launch"] / max(NCU_TRAFFIC["iterations"], 1)
-            traffic = per_iter * iters
+            # scale the captured launch to this launch's iteration count (the
+            # prologue moves 16n bytes once, the rest grows per iteration)
+            per_iter = (NCU_TRAFFIC["bytes_per_launch"] - 16 * n) / max(NCU_TRAFFIC["iterations"], 1)
+            traffic = 16 * n + per_iter * iters
         line = {
             "metric": "pagerank_gteps",
             "value": edges_iters_all / (t_dev * 1e-3) / 1e9,
