@@ -282,6 +282,9 @@ def main():
     total_ms = sum(step_ms)
     edges_iters = sum(m * s.iterations for s in stats)
     kernel_ms = [s.device_ms for s in stats]
+    # clocks cover the kernel-timed region; the sampler's NVML polling is
+    # stopped before the end-to-end loop so it cannot stall its driver calls
+    clocks = sampler.stop() if sampler else None
 
     # ---- e2e: the C-ABI call from pinned host buffers (build + pagerank)
     h_src = torch.from_numpy(src).pin_memory()
@@ -308,7 +311,6 @@ def main():
         it = e2e_step()
         e2e_times.append(time.perf_counter() - t0)
         e2e_iters.append(it)
-    clocks = sampler.stop() if sampler else None
 
     # ---- max over ranks
     t_dev = total_ms

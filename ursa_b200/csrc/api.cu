@@ -70,7 +70,7 @@ void prepare_device(int device) {
   // the driver after every call.
   cudaMemPool_t pool;
   UG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-  uint64_t threshold = UINT64_MAX;
+  uint64_t threshold = 16ull << 30;  // keep up to 16 GiB of freed blocks for reuse
   UG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
   g_prepared[device] = true;
 }
@@ -121,6 +121,12 @@ TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_
   t->n = n;
   t->m = m;
   build_csr(n, d_src, d_dst, m, t->out, s);
+  // The endpoint columns are on the device in row order right now, so the
+  // transpose is a second stable sort by destination -- the same in-CSR the
+  // lazy reconstruction would produce (topology.rs:343-348), without
+  // un-permuting the out-CSR later.
+  build_csr(n, d_dst, d_src, m, t->in, s);
+  t->has_in = true;
   UG_CUDA(cudaStreamSynchronize(s));
   return t;
 }

@@ -129,24 +129,15 @@ __device__ __forceinline__ bool tight(const unsigned long long* __restrict__ dis
   return du < dv || (du == dv && u < v);  // zero weights: keep the DAG acyclic
 }
 
-// tight in-slot counts over every out-slot (owner by binary search)
+// tight in-slot counts over every out-slot
 __global__ void tight_indeg_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
                               const double* __restrict__ w, uint64_t n, uint64_t m,
                               const unsigned long long* __restrict__ dist,
                               uint32_t* __restrict__ indeg) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-      uint64_t mid = (lo + hi) >> 1;
-      if ((uint64_t)off[mid] <= k)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    uint32_t u = (uint32_t)lo, v = tgt[k];
+  for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) {
+    uint32_t v = tgt[k];
     if (tight(dist, u, v, w[k])) atomicAdd(&indeg[v], 1u);
-  }
+  });
 }
 
 __global__ void kahn_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,

@@ -56,22 +56,13 @@ __global__ void iota_k(uint32_t* p, uint64_t n) {
 }
 
 // One thread per out-edge slot; the owning node comes from a binary search
-// over the offsets, restricted to the block's node range.
+// over the offsets, restricted to the rows overlapping the block's slots.
 __global__ void union_edges_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
                               uint64_t n, uint64_t m, uint32_t* parent) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-      uint64_t mid = (lo + hi) >> 1;
-      if ((uint64_t)off[mid] <= k)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    uint32_t u = (uint32_t)lo, v = tgt[k];
+  for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) {
+    uint32_t v = tgt[k];
     if (u != v) unite(parent, u, v);
-  }
+  });
 }
 
 __global__ void flatten_k(uint32_t* parent, uint64_t n, uint32_t* __restrict__ out) {

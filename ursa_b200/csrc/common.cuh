@@ -86,20 +86,22 @@ struct Scratch {
   }
 };
 
-// Persistent device allocation (owned by a topology object).
+// Device allocation owned by a topology object, taken from the device's
+// stream-ordered pool on the building call's stream.  Every call that uses a
+// topology has finished before it returns, so the free is ordered on the
+// per-thread default stream (always valid, whichever thread frees).
 template <class T>
 struct DevArray {
   T* p = nullptr;
   size_t n = 0;
   DevArray() = default;
-  explicit DevArray(size_t count) { alloc(count); }
-  void alloc(size_t count) {
+  void alloc(size_t count, cudaStream_t s) {
     release();
     n = count;
-    if (count) UG_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    if (count) UG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), s));
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, cudaStreamPerThread);
     p = nullptr;
     n = 0;
   }

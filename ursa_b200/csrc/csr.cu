@@ -19,25 +19,9 @@ namespace ug {
 
 namespace {
 
-__device__ __forceinline__ uint32_t owner_of(const uint32_t* __restrict__ off, uint64_t n,
-                                             uint64_t k) {
-  // largest u in [0, n) with off[u] <= k
-  uint64_t lo = 0, hi = n;  // answer in [lo, hi)
-  while (hi - lo > 1) {
-    uint64_t mid = (lo + hi) >> 1;
-    if ((uint64_t)off[mid] <= k)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return (uint32_t)lo;
-}
-
 __global__ void owners_k(const uint32_t* __restrict__ off, uint64_t n, uint64_t m,
                          uint32_t* __restrict__ owner) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x)
-    owner[k] = owner_of(off, n, k);
+  for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) { owner[k] = u; });
 }
 
 // reconstruct_endpoints (topology.rs:307-321) in one pass: slot k of node u
@@ -45,26 +29,24 @@ __global__ void owners_k(const uint32_t* __restrict__ off, uint64_t n, uint64_t 
 __global__ void unpermute_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
                             const uint32_t* __restrict__ eid, uint64_t n, uint64_t m,
                             uint32_t* __restrict__ src_by_row, uint32_t* __restrict__ dst_by_row) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x) {
+  for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) {
     uint32_t r = eid[k];
-    src_by_row[r] = owner_of(off, n, k);
+    src_by_row[r] = u;
     dst_by_row[r] = tgt[k];
-  }
+  });
 }
 
 __global__ void und_pairs_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
                             uint64_t n, uint64_t m, uint32_t* __restrict__ first,
                             uint32_t* __restrict__ second) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t u = owner_of(off, n, k), v = tgt[k];
+  for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) {
+    uint32_t v = tgt[k];
     bool self = u == v;
     first[2 * k] = self ? (uint32_t)n : u;
     second[2 * k] = v;
     first[2 * k + 1] = self ? (uint32_t)n : v;
     second[2 * k + 1] = u;
-  }
+  });
 }
 
 __global__ void und_flags_k(const uint32_t* __restrict__ first, const uint32_t* __restrict__ second,
@@ -105,9 +87,9 @@ void csr_owners(const uint32_t* off, uint64_t n, uint64_t m, uint32_t* owner, cu
 
 void build_csr(uint64_t n, const uint32_t* d_keys, const uint32_t* d_other, uint64_t m,
                DevCsr& out, cudaStream_t s) {
-  out.off.alloc(n + 1);
-  out.tgt.alloc(m);
-  out.eid.alloc(m);
+  out.off.alloc(n + 1, s);
+  out.tgt.alloc(m, s);
+  out.eid.alloc(m, s);
   if (m == 0) {
     UG_CUDA(cudaMemsetAsync(out.off.get(), 0, (n + 1) * sizeof(uint32_t), s));
     return;
@@ -143,10 +125,10 @@ void ensure_undirected(TopoImpl* t, cudaStream_t s) {
   uint64_t len = 2 * m;
   UG_CHECK(len < (1ull << 32), URSA_GPU_EINVAL,
            "undirected CSR build: 2 * n_edges must be below 2^32");
-  t->und_off.alloc(n + 1);
+  t->und_off.alloc(n + 1, s);
   if (m == 0) {
     UG_CUDA(cudaMemsetAsync(t->und_off.get(), 0, (n + 1) * sizeof(uint32_t), s));
-    t->und_tgt.alloc(0);
+    t->und_tgt.alloc(0, s);
     t->m_und = 0;
     UG_CUDA(cudaStreamSynchronize(s));
     t->has_und = true;
@@ -171,7 +153,7 @@ void ensure_undirected(TopoImpl* t, cudaStream_t s) {
   uint32_t m_und = 0;
   UG_CUDA(cudaMemcpyAsync(&m_und, total.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaStreamSynchronize(s));
-  t->und_tgt.alloc(m_und);
+  t->und_tgt.alloc(m_und, s);
   Scratch<uint32_t> ufirst(m_und, s);
   if (m_und) {
     und_compact_k<<<grid_for(len), kBlock, 0, s>>>(first.get(), second.get(), flag.get(),
@@ -188,7 +170,7 @@ void ensure_undirected(TopoImpl* t, cudaStream_t s) {
 void ensure_outdeg(TopoImpl* t, cudaStream_t s) {
   std::lock_guard<std::mutex> g(t->mu);
   if (t->has_outdeg) return;
-  t->outdeg.alloc(t->n);
+  t->outdeg.alloc(t->n, s);
   if (t->n) {
     degree_k<<<grid_for(t->n), kBlock, 0, s>>>(t->out.off.get(), t->n, t->outdeg.get());
     UG_LAUNCH_CHECK();

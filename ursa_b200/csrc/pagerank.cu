@@ -104,21 +104,12 @@ __global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n,
                                const uint32_t* __restrict__ in_src,
                                const uint32_t* __restrict__ in_eid, uint32_t* __restrict__ src_new,
                                uint32_t* __restrict__ eid_new) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-      uint64_t mid = (lo + hi) >> 1;
-      if ((uint64_t)off_new[mid] <= k)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    uint32_t u = old_of_new[lo];
-    uint32_t slot = in_off[u] + (uint32_t)(k - off_new[lo]);
+  for_each_slot_owner(off_new, n, m, [&](uint64_t k, uint32_t i) {
+    uint32_t u = old_of_new[i];
+    uint32_t slot = in_off[u] + (uint32_t)(k - off_new[i]);
     src_new[k] = new_of_old[in_src[slot]];
     eid_new[k] = in_eid[slot];
-  }
+  });
 }
 
 // Class boundaries over the non-increasing degree sequence: bounds[t] =
@@ -522,13 +513,13 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
     Scratch<uint32_t> key(n, s), key_sorted(n, s);
     neg_indeg_k<<<grid_for(n), kBlock, 0, s>>>(t->in.off.get(), n, key.get());
     UG_LAUNCH_CHECK();
-    plan->old_of_new.alloc(n);
+    plan->old_of_new.alloc(n, s);
     radix_sort_pairs(key.get(), nullptr, n, 32, key_sorted.get(), plan->old_of_new.get(), nullptr,
                      nullptr, s);
   }
-  plan->new_of_old.alloc(n);
-  plan->outdeg.alloc(n);
-  plan->off.alloc(n + 1);
+  plan->new_of_old.alloc(n, s);
+  plan->outdeg.alloc(n, s);
+  plan->off.alloc(n + 1, s);
   Scratch<uint32_t> deg(n + 1, s);
   relabel_maps_k<<<grid_for(n), kBlock, 0, s>>>(plan->old_of_new.get(), n, t->in.off.get(),
                                                  t->out.off.get(), plan->new_of_old.get(),
@@ -536,8 +527,8 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   UG_LAUNCH_CHECK();
   UG_CUDA(cudaMemsetAsync(deg.get() + n, 0, sizeof(uint32_t), s));
   exclusive_scan_u32(deg.get(), plan->off.get(), n + 1, nullptr, s);
-  plan->src.alloc(m ? m : 1);
-  plan->eid.alloc(m ? m : 1);
+  plan->src.alloc(m ? m : 1, s);
+  plan->eid.alloc(m ? m : 1, s);
   if (m) {
     relabel_copy_k<<<grid_for(m), kBlock, 0, s>>>(plan->off.get(), n, m, plan->old_of_new.get(),
                                                    plan->new_of_old.get(), t->in.off.get(),
@@ -563,8 +554,8 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   }
   plan->n_hub = c.hi[0];
   // hub chunks
-  plan->hub_nch.alloc(plan->n_hub ? plan->n_hub : 1);
-  plan->hub_first.alloc(plan->n_hub ? plan->n_hub : 1);
+  plan->hub_nch.alloc(plan->n_hub ? plan->n_hub : 1, s);
+  plan->hub_first.alloc(plan->n_hub ? plan->n_hub : 1, s);
   uint32_t n_chunks = 0;
   if (plan->n_hub) {
     Scratch<uint32_t> tot(1, s);
@@ -575,7 +566,7 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
     UG_CUDA(cudaStreamSynchronize(s));
   }
   plan->n_chunks = n_chunks;
-  plan->hub_unit.alloc(n_chunks ? n_chunks : 1);
+  plan->hub_unit.alloc(n_chunks ? n_chunks : 1, s);
   if (n_chunks) {
     hub_units_k<<<grid_for(plan->n_hub), kBlock, 0, s>>>(plan->hub_first.get(), plan->hub_nch.get(),
                                                          plan->n_hub, plan->hub_unit.get());

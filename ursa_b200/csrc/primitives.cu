@@ -177,8 +177,11 @@ __global__ void __launch_bounds__(kBlock) radix_downsweep_k(
     dr[i] = (d << 16) | (before + rank_in);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < 256; d += kBlock) {
-    uint32_t run = 0;
+  // Per digit: each warp's exclusive start, and the tile's digit total.
+  static_assert(kBlock == 256, "one thread per digit");
+  uint32_t run = 0;
+  {
+    const int d = threadIdx.x;
 #pragma unroll
     for (int ww = 0; ww < kWarps; ww++) {
       uint32_t x = wcnt[ww][d];
@@ -186,16 +189,32 @@ __global__ void __launch_bounds__(kBlock) radix_downsweep_k(
       run += x;
     }
   }
+  // Tile-local digit starts, so the tile can be ordered in shared memory and
+  // written out in coalesced runs (one run per digit).
+  __shared__ uint32_t toff[256];
+  __shared__ uint32_t sk[kRadixTile];
+  __shared__ uint32_t sv[kRadixTile];
+  toff[threadIdx.x] = block_exclusive_scan<uint32_t>(run, nullptr);
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kRadixItems; i++) {
     uint32_t d = dr[i] >> 16;
     if (d < 256u) {
-      uint32_t dest = gofs[d] + wcnt[w][d] + (dr[i] & 0xffffu);
-      keys_out[dest] = k[i];
-      vals_out[dest] = v[i];
-      if (gather_src) gather_out[dest] = gather_src[v[i]];
+      uint32_t p = toff[d] + wcnt[w][d] + (dr[i] & 0xffffu);
+      sk[p] = k[i];
+      sv[p] = v[i];
     }
+  }
+  __syncthreads();
+  const uint64_t tile0 = (uint64_t)tile * kRadixTile;
+  const uint32_t tile_n = (uint32_t)(n - tile0 < (uint64_t)kRadixTile ? n - tile0 : kRadixTile);
+  for (uint32_t i = threadIdx.x; i < tile_n; i += kBlock) {
+    const uint32_t key = sk[i], val = sv[i];
+    const uint32_t d = (key >> shift) & mask;
+    const uint32_t dest = gofs[d] + (i - toff[d]);
+    keys_out[dest] = key;
+    vals_out[dest] = val;
+    if (gather_src) gather_out[dest] = gather_src[val];
   }
 }
 

@@ -15,35 +15,18 @@ namespace ug {
 
 namespace {
 
-__device__ __forceinline__ uint32_t owner_u32(const uint32_t* __restrict__ off, uint64_t n,
-                                              uint64_t k) {
-  uint64_t lo = 0, hi = n;
-  while (hi - lo > 1) {
-    uint64_t mid = (lo + hi) >> 1;
-    if ((uint64_t)off[mid] <= k)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return (uint32_t)lo;
-}
-
 __device__ __forceinline__ bool rank_less(uint32_t du, uint32_t u, uint32_t dv, uint32_t v) {
   return du < dv || (du == dv && u < v);
 }
 
 __global__ void orient_flags_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
                                uint64_t n, uint64_t ms, uint32_t* __restrict__ flag) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k <= ms;
-       k += (uint64_t)gridDim.x * blockDim.x) {
-    if (k == ms) {
-      flag[k] = 0u;
-      continue;
-    }
-    uint32_t u = owner_u32(off, n, k), v = tgt[k];
+  if (blockIdx.x == 0 && threadIdx.x == 0) flag[ms] = 0u;
+  for_each_slot_owner(off, n, ms, [&](uint64_t k, uint32_t u) {
+    uint32_t v = tgt[k];
     uint32_t du = off[u + 1] - off[u], dv = off[v + 1] - off[v];
     flag[k] = rank_less(du, u, dv, v) ? 1u : 0u;
-  }
+  });
 }
 
 __global__ void orient_fill_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
@@ -58,11 +41,14 @@ __global__ void orient_fill_k(const uint32_t* __restrict__ off, const uint32_t* 
     o_off[u] = pos[off[u]];
 }
 
+// Threads run independently (intersections vary widely in length), so the
+// owner search here is a plain per-slot binary search.
 __global__ void count_k(const uint32_t* __restrict__ o_off, const uint32_t* __restrict__ o_tgt,
                         uint64_t n, uint64_t mo, uint32_t* __restrict__ tri) {
   for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < mo;
        q += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t u = owner_u32(o_off, n, q), v = o_tgt[q];
+    uint32_t u = owner_of(o_off, n, q);
+    uint32_t v = o_tgt[q];
     uint32_t i = o_off[u], ie = o_off[u + 1];
     uint32_t j = o_off[v], je = o_off[v + 1];
     uint32_t c = 0;
@@ -111,7 +97,7 @@ void triangle_count_run(TopoImpl* t, uint32_t* d_tri, cudaStream_t s) {
   UG_CUDA(cudaMemsetAsync(d_tri, 0, n * sizeof(uint32_t), s));
   if (ms == 0) return;
   Scratch<uint32_t> pos(ms + 1, s);
-  orient_flags_k<<<grid_for(ms + 1), kBlock, 0, s>>>(t->und_off.get(), t->und_tgt.get(), n, ms,
+  orient_flags_k<<<grid_for(ms), kBlock, 0, s>>>(t->und_off.get(), t->und_tgt.get(), n, ms,
                                                      pos.get());
   UG_LAUNCH_CHECK();
   Scratch<uint32_t> total(1, s);
