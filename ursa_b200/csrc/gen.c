@@ -372,6 +372,77 @@ void ug_weights_f32(uint64_t m, float lo, float hi, uint64_t seed, float *out,
   par(m, threads, w_range, &c);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Batches of small R-MAT graphs.  Graph i has n_i nodes, R-MAT on scale      */
+/* ceil(log2 n_i) with edge_factor_i * n_i draws and seed seed0 + i; draws    */
+/* with an endpoint >= n_i are rejected, then self-loops and duplicates are   */
+/* dropped (first occurrence kept).  Edges are written graph after graph with */
+/* local node ids.                                                            */
+typedef struct {
+  const uint64_t *n, *ef, *edge_off;
+  uint64_t seed0;
+  double t0, t1, t2;
+  uint32_t *src, *dst;
+  uint64_t *kept;
+} rbatch_ctx;
+
+static int ceil_log2(uint64_t n) {
+  int s = 0;
+  while ((1ull << s) < n) s++;
+  return s;
+}
+
+static void rbatch_range(void *p, uint64_t lo, uint64_t hi, int tid) {
+  rbatch_ctx *c = (rbatch_ctx *)p;
+  (void)tid;
+  for (uint64_t g = lo; g < hi; g++) {
+    uint64_t n = c->n[g], draws = c->ef[g] * n;
+    int scale = ceil_log2(n);
+    uint64_t seed = c->seed0 + g;
+    uint64_t s = fmix(seed ^ 0xA0761D6478BD642Full);
+    uint32_t *rs = (uint32_t *)malloc((draws ? draws : 1) * sizeof(uint32_t));
+    uint32_t *rd = (uint32_t *)malloc((draws ? draws : 1) * sizeof(uint32_t));
+    uint64_t k = 0;
+    for (uint64_t i = 0; i < draws; i++) {
+      uint32_t u = 0, v = 0;
+      for (int L = 0; L < scale; L++) {
+        double r = unit(fmix(s + (i * 64u + (uint64_t)L + 1u) * GOLDEN));
+        uint32_t bu = r >= c->t1, bv = (r >= c->t0 && r < c->t1) || r >= c->t2;
+        u = (u << 1) | bu;
+        v = (v << 1) | bv;
+      }
+      if (u < n && v < n) {
+        rs[k] = u;
+        rd[k] = v;
+        k++;
+      }
+    }
+    uint64_t kept = ug_dedup(rs, rd, k, c->src + c->edge_off[g], c->dst + c->edge_off[g], 1);
+    c->kept[g] = kept;
+    free(rs);
+    free(rd);
+  }
+}
+
+/* Fills per-graph edges into src/dst at edge_off[g] (capacity ef*n each) and
+ * writes the kept counts; the caller compacts. */
+void ug_rmat_batch(uint64_t count, const uint64_t *n, const uint64_t *ef, uint64_t seed0,
+                   double a, double b, double c, const uint64_t *edge_off, uint32_t *src,
+                   uint32_t *dst, uint64_t *kept, int threads) {
+  rbatch_ctx x;
+  x.n = n;
+  x.ef = ef;
+  x.edge_off = edge_off;
+  x.seed0 = seed0;
+  x.t0 = a;
+  x.t1 = a + b;
+  x.t2 = a + b + c;
+  x.src = src;
+  x.dst = dst;
+  x.kept = kept;
+  par(count, threads, rbatch_range, &x);
+}
+
 /* Uniform 64-bit draws (used for seeded source/query streams). */
 uint64_t ug_draw(uint64_t seed, uint64_t index, uint64_t lane) {
   return draw(seed, index, lane & 63u);

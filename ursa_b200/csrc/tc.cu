@@ -89,29 +89,49 @@ __global__ void clustering_k(const uint32_t* __restrict__ off, const uint32_t* _
 
 }  // namespace
 
-void triangle_count_run(TopoImpl* t, uint32_t* d_tri, cudaStream_t s) {
+// Orientation of the undirected CSR (host-synchronising; done once).
+void orient_build(TopoImpl* t, OrientedCsr& o, cudaStream_t s) {
   const uint64_t n = t->n;
-  if (n == 0) return;
   ensure_undirected(t, s);
   const uint64_t ms = t->m_und;
-  UG_CUDA(cudaMemsetAsync(d_tri, 0, n * sizeof(uint32_t), s));
-  if (ms == 0) return;
+  o.off.alloc(n + 1, s);
+  o.mo = 0;
+  if (ms == 0) {
+    UG_CUDA(cudaMemsetAsync(o.off.get(), 0, (n + 1) * sizeof(uint32_t), s));
+    o.tgt.alloc(1, s);
+    return;
+  }
   Scratch<uint32_t> pos(ms + 1, s);
   orient_flags_k<<<grid_for(ms), kBlock, 0, s>>>(t->und_off.get(), t->und_tgt.get(), n, ms,
-                                                     pos.get());
+                                                 pos.get());
   UG_LAUNCH_CHECK();
   Scratch<uint32_t> total(1, s);
   exclusive_scan_u32(pos.get(), pos.get(), ms + 1, total.get(), s);
-  uint32_t mo = read_u32(total.get(), s);
-  Scratch<uint32_t> o_off(n + 1, s), o_tgt(mo ? mo : 1, s);
+  o.mo = read_u32(total.get(), s);
+  o.tgt.alloc(o.mo ? o.mo : 1, s);
   orient_fill_k<<<grid_for(ms), kBlock, 0, s>>>(t->und_off.get(), t->und_tgt.get(), n, ms,
-                                                pos.get(), o_off.get(), o_tgt.get());
+                                                pos.get(), o.off.get(), o.tgt.get());
   UG_LAUNCH_CHECK();
-  if (mo) {
-    count_k<<<grid_for(mo, kBlock, 148u * 64u), kBlock, 0, s>>>(o_off.get(), o_tgt.get(), n, mo,
-                                                                 d_tri);
+}
+
+// Triangle counts from an oriented CSR: kernels only, so it can be captured
+// into a CUDA graph.
+void triangle_count_oriented(const OrientedCsr& o, uint64_t n, uint32_t* d_tri, cudaStream_t s) {
+  UG_CUDA(cudaMemsetAsync(d_tri, 0, n * sizeof(uint32_t), s));
+  if (o.mo) {
+    count_k<<<grid_for(o.mo, kBlock, 148u * 64u), kBlock, 0, s>>>(o.off.get(), o.tgt.get(), n, o.mo,
+                                                                   d_tri);
     UG_LAUNCH_CHECK();
   }
+}
+
+void triangle_count_run(TopoImpl* t, uint32_t* d_tri, cudaStream_t s) {
+  const uint64_t n = t->n;
+  if (n == 0) return;
+  OrientedCsr o;
+  orient_build(t, o, s);
+  triangle_count_oriented(o, n, d_tri, s);
+  UG_CUDA(cudaStreamSynchronize(s));  // o's buffers are released on return
 }
 
 void clustering_run(TopoImpl* t, double* d_out, cudaStream_t s) {

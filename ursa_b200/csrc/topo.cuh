@@ -50,6 +50,18 @@ void ensure_in(TopoImpl* t, cudaStream_t s);
 void ensure_undirected(TopoImpl* t, cudaStream_t s);
 void ensure_outdeg(TopoImpl* t, cudaStream_t s);
 
+// Undirected CSR with every edge kept once, oriented from the lower to the
+// higher (degree, id) rank (triangle counting).
+struct OrientedCsr {
+  DevArray<uint32_t> off, tgt;
+  uint64_t mo = 0;
+};
+void orient_build(TopoImpl* t, OrientedCsr& o, cudaStream_t s);
+void triangle_count_oriented(const OrientedCsr& o, uint64_t n, uint32_t* d_tri, cudaStream_t s);
+void cc_weak_with_parent(TopoImpl* t, uint32_t* parent, uint32_t* d_out, cudaStream_t s);
+TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m,
+                           cudaStream_t s, int device, ursa_gpu_topo** holder);
+
 // Slot -> owning node for a CSR (binary search over offsets), n_slots = m.
 void csr_owners(const uint32_t* off, uint64_t n, uint64_t m, uint32_t* owner, cudaStream_t s);
 

@@ -87,6 +87,42 @@ def weights_f32(m: int, lo: float = 1.0, hi: float = 10.0, seed: int = 3, thread
     return out
 
 
+def batch_sizes(count: int, median: float = 2000.0, sigma: float = 1.0, lo: int = 100, hi: int = 50_000,
+                ef_lo: int = 8, ef_hi: int = 32, seed: int = 100):
+    """Node counts log-normal(median, sigma) clipped to [lo, hi] and integer
+    edge factors uniform in [ef_lo, ef_hi], from numpy's seeded PCG64."""
+    rng = np.random.default_rng(seed)
+    n = np.clip(np.rint(median * np.exp(sigma * rng.standard_normal(count))), lo, hi).astype(np.uint64)
+    ef = rng.integers(ef_lo, ef_hi + 1, count).astype(np.uint64)
+    return n, ef
+
+
+def rmat_batch(count: int, median: float = 2000.0, sigma: float = 1.0, lo: int = 100, hi: int = 50_000,
+               ef_lo: int = 8, ef_hi: int = 32, seed0: int = 100, abc=RMAT_ABC, threads: int | None = None):
+    """A batch of small R-MAT graphs: graph i has n_i nodes (batch_sizes),
+    R-MAT on scale ceil(log2 n_i) with ef_i * n_i draws and seed seed0 + i,
+    endpoints >= n_i rejected, self-loops and duplicates dropped.  Returns
+    (n[count], edge_counts[count], src, dst) with local ids, graph after graph."""
+    L = _load()
+    n, ef = batch_sizes(count, median, sigma, lo, hi, ef_lo, ef_hi, seed0)
+    cap = (n * ef).astype(np.uint64)
+    off = np.zeros(count + 1, np.uint64)
+    np.cumsum(cap, out=off[1:])
+    src = np.empty(int(off[-1]), np.uint32)
+    dst = np.empty(int(off[-1]), np.uint32)
+    kept = np.empty(count, np.uint64)
+    P = C.c_void_p
+    L.ug_rmat_batch.restype = None
+    L.ug_rmat_batch.argtypes = [C.c_uint64, P, P, C.c_uint64, C.c_double, C.c_double, C.c_double, P, P, P, P,
+                                C.c_int]
+    L.ug_rmat_batch(count, n.ctypes.data, ef.ctypes.data, seed0, abc[0], abc[1], abc[2], off.ctypes.data,
+                    src.ctypes.data, dst.ctypes.data, kept.ctypes.data, _threads(threads))
+    keep = np.zeros(src.size, bool)
+    for g in range(count):
+        keep[int(off[g]):int(off[g] + kept[g])] = True
+    return n, kept, src[keep], dst[keep]
+
+
 def draw(seed: int, index: int, lane: int = 0) -> int:
     """The generators' counter-based 64-bit draw."""
     return int(_load().ug_draw(seed, index, lane))
