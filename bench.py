@@ -21,6 +21,18 @@ no L2 flush is needed between steps.
 Multi-GPU (--gpus N under torchrun): replicas only (each rank runs the whole
 workload on its own GPU, no collective on the data path); value sums ranks'
 edges x iterations over the max time across ranks.
+
+--workload batch: 10,000 uneven R-MAT graphs (node counts log-normal, median
+2,000, clipped to [100, 50,000]; per-graph edge factor uniform in [8, 32];
+seed 100 + i; see ursa_b200.gen.rmat_batch).  A step is pagerank (d 0.85,
+tol 1e-6, max_iter 100), weak components and triangle counts for every graph
+in one launch of the batch's captured CUDA graph (bucket and tile shapes
+autotuned once before timing).  value = graphs/s of that launch (device
+time); e2e = the public API from pinned host buffers per step (batch build
+with the H2D of every edge row, the launch, the D2H of every result); beside
+them the per-graph plain loop -- one topology and one pagerank /
+connected_components_weak / triangle_count call per graph -- timed over the
+whole batch with topologies resident, and with builds.
 """
 
 from __future__ import annotations
@@ -203,12 +215,250 @@ def cpu_baseline(n, src, dst):
             "sample": f"{iters} warm power iterations (tol=0) on the same R-MAT-22 graph, CSR+transpose prebuilt"}
 
 
+BATCH_COUNT = 10_000
+BATCH_WORKLOAD = "rmat_batch10k_pr_cc_tc"
+
+
+def batch_pagerank_bytes(n, m, iters) -> int:
+    """Compulsory bytes of the batch's pagerank phase: per graph and
+    iteration 4m (in-CSR sources) + 4(n+1) (offsets) + 4n (out-degree) + 8n
+    (old rank) + 8n (new rank) + 4n (new share) = 4m + 28n + 4."""
+    return int(np.sum(iters.astype(np.int64) * (4 * m + 28 * n + 4)))
+
+
+def batch_graphs(count=BATCH_COUNT):
+    from ursa_b200 import gen
+
+    n, k, s, d = gen.rmat_batch(count)
+    return n, k, s, d
+
+
+def batch_cpu_sample(n, k, s, d, sample=64):
+    """The oracle (CPU restatement of ursa-core) on a bounded, evenly spaced
+    sample of the batch: topology build + pagerank + components + triangle
+    count per graph, all host threads; returned as graphs/s."""
+    from oracle import oracle as O
+
+    O.build()
+    O.set_threads(os.cpu_count() or 1)
+    off = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
+    idx = np.linspace(0, len(n) - 1, sample).astype(int)
+    t0 = time.perf_counter()
+    for i in idx:
+        t = O.Topology(int(n[i]), s[off[i]:off[i + 1]], d[off[i]:off[i + 1]])
+        O.pagerank(t, DAMPING, MAX_ITER, TOL)
+        O.connected_components_weak(t)
+        O.triangle_count(t)
+    dt = time.perf_counter() - t0
+    # scale by edges: the sample's share of the batch's edge rows
+    frac = float(k[idx].sum()) / float(k.sum())
+    per_batch_s = dt / frac
+    return {"value": len(n) / per_batch_s, "unit": "graphs/s", "cores": O.get_threads(), "kind": "port",
+            "sample": f"{sample} evenly spaced graphs of the batch (build + pagerank + components + triangles), "
+                      f"scaled to the whole batch by edge rows ({100 * frac:.2f}% of them)"}
+
+
+def run_reference_batch(args, rank, world):
+    """The reference algorithm on the host for the batch workload: per step a
+    bounded, evenly spaced sample of the batch through the oracle."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    O.build()
+    O.set_threads(os.cpu_count() or 1)
+    n, k, s, d = batch_graphs()
+    for _ in range(args.warmup):
+        batch_cpu_sample(n, k, s, d, sample=16)
+    vals = [batch_cpu_sample(n, k, s, d) for _ in range(args.steps)]
+    value = statistics.median(v["value"] for v in vals)
+    cb = dict(vals[-1])
+    cb["value"] = value
+    line = {
+        "impl": "reference",
+        "metric": "batch_graphs_per_s",
+        "value": value,
+        "unit": "graphs/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * len(n) / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "graphs": len(n), "n_nodes": int(n.sum()), "n_edges": int(k.sum()),
+                   "damping": DAMPING, "tol": TOL, "max_iter": MAX_ITER},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args, rank, world):
+    import torch
+
+    local_rank = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    from ursa_b200 import PageRankParams, Topology, _lib, algo
+    from ursa_b200.batch import GraphBatch
+
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(local_rank))
+    n, k, s, d = batch_graphs()
+    G, N, M = len(n), int(n.sum()), int(k.sum())
+    params = PageRankParams(DAMPING, MAX_ITER, TOL)
+    h_s = torch.from_numpy(s).pin_memory()
+    h_d = torch.from_numpy(d).pin_memory()
+    nn, kk = np.ascontiguousarray(n, np.uint64), np.ascontiguousarray(k, np.uint64)
+
+    def build():
+        h = C.c_void_p()
+        _lib.check(L.ursa_gpu_batch_build(G, nn.ctypes.data, kk.ctypes.data, h_s.data_ptr(), h_d.data_ptr(),
+                                          C.byref(h)))
+        return h
+
+    b = GraphBatch(n, k, s, d)
+    cfg, tuned_ms = b.tune(params)
+    stream = torch.cuda.Stream()
+    for _ in range(max(args.warmup, 3)):
+        b.run(params, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    launches0 = L.ursa_gpu_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        b.run(params, stream=stream.cuda_stream)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    launches = L.ursa_gpu_launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    step_ms = [a.elapsed_time(c) for a, c in ev]
+    res = b.results()
+    iters = res.iterations
+    # per-algorithm device time (one launch each, after the timed region)
+    split = {}
+    from ursa_b200.batch import BATCH_COMPONENTS, BATCH_PAGERANK, BATCH_TRIANGLES
+
+    for name, what in (("pagerank", BATCH_PAGERANK), ("components", BATCH_COMPONENTS),
+                       ("triangles", BATCH_TRIANGLES)):
+        b.run(params, what=what)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(params, what=what, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        split[name] = e0.elapsed_time(e1)
+    b.run(params)
+    b_bytes = b.device_bytes()
+    b.close()
+
+    # e2e through the public API: build (H2D) + launch + results (D2H)
+    h_pr = torch.empty(N, dtype=torch.float64).pin_memory()
+    h_cc = torch.empty(N, dtype=torch.int32).pin_memory()
+    h_tc = torch.empty(N, dtype=torch.int32).pin_memory()
+    h_it = torch.empty(G, dtype=torch.int32).pin_memory()
+    h_de = torch.empty(G, dtype=torch.float64).pin_memory()
+    cfg_c = _lib.BatchConfig()
+    cfg_c.n_buckets = cfg["n_buckets"]
+    for i in range(cfg["n_buckets"]):
+        cfg_c.cap[i], cfg_c.threads[i] = cfg["cap"][i], cfg["threads"][i]
+    cfg_c.tc_tile, cfg_c.tc_threads = cfg["tc_tile"], cfg["tc_threads"]
+    e2e = []
+    for i in range(max(1, min(args.steps, 3)) + 1):
+        t0 = time.perf_counter()
+        h = build()
+        try:
+            _lib.check(L.ursa_gpu_batch_set_config(h, C.byref(cfg_c)))
+            _lib.check(L.ursa_gpu_batch_run(h, C.byref(params), 7, None))
+            _lib.check(L.ursa_gpu_batch_results(h, h_pr.data_ptr(), h_cc.data_ptr(), h_tc.data_ptr(),
+                                                h_it.data_ptr(), h_de.data_ptr()))
+        finally:
+            L.ursa_gpu_batch_free(h)
+        if i:  # the first pass warms the pool
+            e2e.append(time.perf_counter() - t0)
+
+    # the per-graph plain loop over the same graphs
+    off = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
+    t0 = time.perf_counter()
+    tops = [Topology.build(int(n[i]), s[off[i]:off[i + 1]], d[off[i]:off[i + 1]]) for i in range(G)]
+    plain_build_s = time.perf_counter() - t0
+
+    def plain_pass():
+        for t in tops:
+            algo.pagerank(t, params)
+            algo.connected_components_weak(t)
+            algo.triangle_count(t)
+
+    plain_pass()  # plans, lazily built CSRs, pool
+    t0 = time.perf_counter()
+    plain_pass()
+    plain_s = time.perf_counter() - t0
+    del tops
+
+    if rank == 0:
+        ms = statistics.median(step_ms)
+        pr_bytes = batch_pagerank_bytes(n.astype(np.int64), k.astype(np.int64), iters)
+        pr_achieved = pr_bytes / (split["pagerank"] * 1e-3) / 1e9
+        peak, peak_kind = load_peaks()
+        line = {
+            "metric": "batch_graphs_per_s",
+            "value": G / (ms * 1e-3),
+            "unit": "graphs/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32-compensated SpMV, f64 ranks/residual; u32 components and triangle counts",
+            "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "graphs": G, "n_nodes": N, "n_edges": M,
+                       "damping": DAMPING, "tol": TOL, "max_iter": MAX_ITER,
+                       "pagerank_iterations": {"min": int(iters.min()), "median": float(np.median(iters)),
+                                               "max": int(iters.max()), "sum": int(iters.sum())},
+                       "tuned": cfg, "tuned_ms": tuned_ms, "device_bytes": b_bytes,
+                       "l2": "inputs larger than L2 (in-CSR 1.9 GB)"},
+            "split_ms": split,
+            "e2e": {"value": G / statistics.median(e2e), "unit": "graphs/s",
+                    "h2d_bytes_per_step": 8 * M + 16 * G, "d2h_bytes_per_step": 16 * N + 12 * G,
+                    "ms_per_step": 1e3 * statistics.median(e2e)},
+            "plain_loop": {"graphs_per_s": G / plain_s, "s": plain_s, "build_s": plain_build_s,
+                           "e2e_graphs_per_s": G / (plain_s + plain_build_s),
+                           "calls": "Topology per graph; pagerank + connected_components_weak + "
+                                    "triangle_count per graph, host outputs"},
+            "speedup_vs_plain": {"device": (G / (ms * 1e-3)) / (G / plain_s),
+                                 "e2e": (G / statistics.median(e2e)) / (G / (plain_s + plain_build_s))},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "batch_k (pagerank-only launch)", "achieved": pr_achieved,
+                         "peak": peak, "unit": "GB/s", "frac": pr_achieved / peak, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes_per_launch": pr_bytes,
+                         "note": "triangle counting (most of the step) is intersection-bound, not HBM-bound"},
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = batch_cpu_sample(n, k, s, d)
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
@@ -218,7 +468,13 @@ def main():
     local_rank = env_int("LOCAL_RANK", 0)
 
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        if args.workload == "batch":
+            run_reference_batch(args, rank, world)
+        else:
+            run_reference(args, rank, world)
+        return
+    if args.workload == "batch":
+        run_batch(args, rank, world)
         return
 
     import torch

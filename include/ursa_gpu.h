@@ -214,6 +214,87 @@ int ursa_gpu_betweenness_weighted(ursa_gpu_topo *t, const double *weights, uint6
                                   int has_sample, double sample, int has_seed, uint64_t seed,
                                   double *out);
 
+/* ------------------------------------------------------------------------
+ * Batched execution of many small independent graphs.
+ *
+ * The reference runs one graph per Topology: Topology::build
+ * (topology.rs:276-298) and then pagerank (algo/pagerank.rs:98-124),
+ * connected_components_weak (algo/components.rs:58-68) and triangle_count
+ * (algo/triangle.rs:40-62), each call on its own.  A batch holds thousands
+ * of graphs on the device at once and runs all three for every graph in ONE
+ * launch of a captured CUDA graph; per graph the results equal those of the
+ * single-graph calls above (pagerank within the same tolerance, components
+ * and triangle counts exactly), and they do not depend on the batch's other
+ * graphs or on the launch configuration.
+ * ---------------------------------------------------------------------- */
+typedef struct ursa_gpu_batch ursa_gpu_batch;
+
+enum {
+  URSA_GPU_BATCH_PAGERANK = 1,
+  URSA_GPU_BATCH_COMPONENTS = 2,
+  URSA_GPU_BATCH_TRIANGLES = 4
+};
+
+/* Launch shapes of a batch (bucket and tile shapes).  Pagerank and
+ * components run per graph: a graph runs in the first bucket whose capacity
+ * (nodes) holds it, and graphs above the last capacity run in the last
+ * bucket with their per-node state in global memory; threads: CTA size per
+ * bucket (128, 256, 512 or 1024).  Capacities rise and are at most 57,344
+ * nodes (224 KB of shared memory per CTA).  Triangle counting runs over the
+ * whole batch: warps take tc_tile consecutive vertices of a graph at a time
+ * (1..4096), in CTAs of tc_threads (128, 256 or 512). */
+typedef struct {
+  uint32_t n_buckets; /* 1..3 */
+  uint32_t cap[3];
+  uint32_t threads[3];
+  uint32_t tc_tile;
+  uint32_t tc_threads;
+} ursa_gpu_batch_config;
+
+/* Uploads a batch: graph g has node_counts[g] nodes and edge_counts[g] edge
+ * rows; src/dst hold every graph's rows one graph after another, with LOCAL
+ * ids (0 <= id < node_counts[g]) -- per graph the (n, src, dst) of
+ * Topology::build.  Totals are limited to u32::MAX nodes and edges.  Builds
+ * the union's in-CSR, out-degrees and oriented undirected CSR, and groups
+ * each graph's rows by in-degree.  Uses the device selected with
+ * ursa_gpu_set_device. */
+int ursa_gpu_batch_build(uint64_t n_graphs, const uint64_t *node_counts,
+                         const uint64_t *edge_counts, const uint32_t *src, const uint32_t *dst,
+                         ursa_gpu_batch **out);
+void ursa_gpu_batch_free(ursa_gpu_batch *b);
+uint64_t ursa_gpu_batch_n_graphs(const ursa_gpu_batch *b);
+uint64_t ursa_gpu_batch_n_nodes(const ursa_gpu_batch *b);
+uint64_t ursa_gpu_batch_n_edges(const ursa_gpu_batch *b);
+uint64_t ursa_gpu_batch_device_bytes(const ursa_gpu_batch *b);
+
+/* Runs the algorithms selected by `what` (URSA_GPU_BATCH_* flags) for every
+ * graph as one CUDA-graph launch (captured on the first call and again
+ * whenever params, `what` or the configuration change).  params: pagerank's
+ * PageRankParams (pagerank.rs:22-36).  stream: a cudaStream_t to enqueue on
+ * and return at once, or NULL for this thread's stream and return when
+ * done. */
+int ursa_gpu_batch_run(ursa_gpu_batch *b, const ursa_gpu_pagerank_params *params, uint32_t what,
+                       void *stream);
+
+/* Autotuner: times the captured launch for a set of bucket capacities, CTA
+ * sizes per bucket and triangle tiles (coordinate search, min of two timed
+ * launches each) and keeps the fastest.  Writes the choice and its time when
+ * the pointers are non-NULL.  Results do not change with the choice. */
+int ursa_gpu_batch_tune(ursa_gpu_batch *b, const ursa_gpu_pagerank_params *params, uint32_t what,
+                        ursa_gpu_batch_config *chosen, float *best_ms);
+int ursa_gpu_batch_set_config(ursa_gpu_batch *b, const ursa_gpu_batch_config *cfg);
+int ursa_gpu_batch_get_config(ursa_gpu_batch *b, ursa_gpu_batch_config *cfg);
+
+/* Results of the last run (the copy waits for it, on any stream),
+ * concatenated graph after graph in node order (any pointer may be NULL): pagerank f64 and component labels (minimum
+ * member LOCAL id) and triangle counts u32, n_nodes each; per graph the
+ * pagerank iteration count and last L1 delta, n_graphs each. */
+int ursa_gpu_batch_results(ursa_gpu_batch *b, double *pagerank, uint32_t *components,
+                           uint32_t *triangles, uint32_t *pr_iterations, double *pr_last_delta);
+/* Device addresses of the same result arrays (valid until ursa_gpu_batch_free). */
+int ursa_gpu_batch_device_results(ursa_gpu_batch *b, const double **pagerank,
+                                  const uint32_t **components, const uint32_t **triangles);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,31 @@ class PageRankStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("last_delta", C.c_double), ("device_ms", C.c_double)]
 
 
+class BatchConfig(C.Structure):
+    """ursa_gpu_batch_config: bucket capacities (nodes) and CTA size per
+    bucket, and the triangle kernel's vertices per warp unit and CTA size."""
+
+    _fields_ = [
+        ("n_buckets", C.c_uint32),
+        ("cap", C.c_uint32 * 3),
+        ("threads", C.c_uint32 * 3),
+        ("tc_tile", C.c_uint32),
+        ("tc_threads", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        nb = self.n_buckets
+        return {
+            "n_buckets": nb,
+            "cap": list(self.cap)[:nb],
+            "threads": list(self.threads)[:nb],
+            "tc_tile": self.tc_tile,
+            "tc_threads": self.tc_threads,
+        }
+
+
+BATCH_PAGERANK, BATCH_COMPONENTS, BATCH_TRIANGLES = 1, 2, 4
+
 # Every exported symbol with its (restype, argtypes).
 P, u32, u64, i32, i64, f64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_int64, C.c_double
 SIGNATURES = {
@@ -82,6 +107,21 @@ SIGNATURES = {
     "ursa_gpu_clustering_coefficient": (i32, [P, P]),
     "ursa_gpu_betweenness": (i32, [P, i32, f64, i32, u64, P]),
     "ursa_gpu_betweenness_weighted": (i32, [P, P, u64, i32, f64, i32, u64, P]),
+    "ursa_gpu_batch_build": (i32, [u64, P, P, P, P, C.POINTER(P)]),
+    "ursa_gpu_batch_free": (None, [P]),
+    "ursa_gpu_batch_n_graphs": (u64, [P]),
+    "ursa_gpu_batch_n_nodes": (u64, [P]),
+    "ursa_gpu_batch_n_edges": (u64, [P]),
+    "ursa_gpu_batch_device_bytes": (u64, [P]),
+    "ursa_gpu_batch_run": (i32, [P, C.POINTER(PageRankParams), u32, P]),
+    "ursa_gpu_batch_tune": (
+        i32,
+        [P, C.POINTER(PageRankParams), u32, C.POINTER(BatchConfig), C.POINTER(C.c_float)],
+    ),
+    "ursa_gpu_batch_set_config": (i32, [P, C.POINTER(BatchConfig)]),
+    "ursa_gpu_batch_get_config": (i32, [P, C.POINTER(BatchConfig)]),
+    "ursa_gpu_batch_results": (i32, [P, P, P, P, P, P]),
+    "ursa_gpu_batch_device_results": (i32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
 }
 
 _lib = None

@@ -2,52 +2,16 @@
 //
 // The reference runs a serial union-find (path halving, union by rank) over
 // the out-edges and labels each node with its representative.  Here every
-// out-edge slot is processed in parallel by a lock-free union-find: a union
-// always hooks the larger root under the smaller one with a compare-and-swap
-// (a failed CAS means the root moved; the walk continues from the new
-// parent), and finds compress paths by pointer jumping.  Parents only ever
-// decrease, so each tree's root is the minimum id of its component, and the
+// out-edge slot is processed in parallel by the lock-free union-find of
+// unionfind.cuh; each tree's root is the minimum id of its component, so the
 // final labels are the minimum member ids: the reference's partition with a
 // canonical representative.
 #include "frontier.cuh"
+#include "unionfind.cuh"
 
 namespace ug {
 
 namespace {
-
-__device__ __forceinline__ uint32_t ld_parent(const uint32_t* p, uint32_t x) {
-  return *(const volatile uint32_t*)&p[x];
-}
-
-// Root of x with intermediate pointer jumping (parent[x] < x off the root).
-__device__ __forceinline__ uint32_t find_root(uint32_t* p, uint32_t x) {
-  uint32_t par = ld_parent(p, x);
-  if (par != x) {
-    uint32_t prev = x, next;
-    while (par > (next = ld_parent(p, par))) {
-      p[prev] = next;
-      prev = par;
-      par = next;
-    }
-  }
-  return par;
-}
-
-__device__ __forceinline__ void unite(uint32_t* p, uint32_t a, uint32_t b) {
-  uint32_t ra = find_root(p, a), rb = find_root(p, b);
-  // bounded by the depth of the forest; each failed CAS moves one link up
-  while (ra != rb) {
-    if (ra < rb) {
-      uint32_t old = atomicCAS(&p[rb], rb, ra);
-      if (old == rb) return;
-      rb = old;
-    } else {
-      uint32_t old = atomicCAS(&p[ra], ra, rb);
-      if (old == ra) return;
-      ra = old;
-    }
-  }
-}
 
 __global__ void iota_k(uint32_t* p, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -61,19 +25,14 @@ __global__ void union_edges_k(const uint32_t* __restrict__ off, const uint32_t* 
                               uint64_t n, uint64_t m, uint32_t* parent) {
   for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) {
     uint32_t v = tgt[k];
-    if (u != v) unite(parent, u, v);
+    if (u != v) uf_unite(parent, u, v);
   });
 }
 
 __global__ void flatten_k(uint32_t* parent, uint64_t n, uint32_t* __restrict__ out) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t x = (uint32_t)i, par = ld_parent(parent, x);
-    while (par != x) {
-      x = par;
-      par = ld_parent(parent, x);
-    }
-    out[i] = par;
+    out[i] = uf_root(parent, (uint32_t)i);
   }
 }
 
