@@ -33,6 +33,17 @@ with the H2D of every edge row, the launch, the D2H of every result); beside
 them the per-graph plain loop -- one topology and one pagerank /
 connected_components_weak / triangle_count call per graph -- timed over the
 whole batch with topologies resident, and with builds.
+
+--workload serve: the serving loop on a resident R-MAT scale-24 graph
+(16,777,216 nodes, edge factor 16, seed 4; out-CSR and transpose resident)
+plus uploaded small graphs (sized as the batch workload) arriving as a
+Poisson stream of 200/s, each kept for 2 s.  Queries arrive as a seeded
+Poisson stream at each swept rate: 50% shortest_path between uniform random
+nodes, 30% hop(k=2) from a uniform random seed, 20% pagerank (d 0.85, tol
+1e-6, max_iter 100) on a live upload.  Per rate: completed queries/s and
+p50/p99 latency (submit to completion, queueing included).  Beside it the
+plain one-query-per-launch path (shortest_path / k_hop / pagerank C-ABI calls
+from 4 host threads, closed loop) over the same queries.
 """
 
 from __future__ import annotations
@@ -296,6 +307,218 @@ def run_reference_batch(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+SERVE_WORKLOAD = "serve_rmat24_uploads"
+SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
+
+
+def serve_queries(n, rng, count):
+    """(kind, a, b) with kind 0 = shortest_path(a, b), 1 = hop(a, k=2),
+    2 = pagerank on the upload picked by b (a uniform draw)."""
+    r = rng.random(count)
+    kind = np.where(r < 0.5, 0, np.where(r < 0.8, 1, 2))
+    a = rng.integers(0, n, count)
+    b = rng.integers(0, n, count)
+    return kind, a, b
+
+
+def run_serve(args, rank, world):
+    import torch
+
+    local_rank = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    from ursa_b200 import PageRankParams, Topology, _lib, algo, gen
+    from ursa_b200.serve import Server
+
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(local_rank))
+    n, src, dst = gen.rmat(24, 16, 4)
+    m = int(src.size)
+    topo = Topology.build(n, src, dst)
+    topo.prepare(transpose=True)
+    del src, dst
+    un, uk, us, ud = gen.rmat_batch(600, seed0=5000)
+    uoff = np.concatenate([[0], np.cumsum(uk)]).astype(np.int64)
+    ups = [(int(un[i]), us[uoff[i]:uoff[i + 1]], ud[uoff[i]:uoff[i + 1]]) for i in range(len(un))]
+    srv = Server(topo, path_lanes=4, path_slots=16, hop_lanes=4, hop_slots=16, pr_lanes=2, pr_slots=32,
+                 pr_max_nodes=65536, hbm_reserve_bytes=16 << 30)
+    live, live_lock = [], threading.Lock()
+    stop_up = threading.Event()
+
+    def uploader():
+        """Poisson(200/s) uploads, each released 2 s after it arrived."""
+        r = np.random.default_rng(77)
+        i = 0
+        held = []
+        t_next = time.perf_counter()
+        while not stop_up.is_set():
+            t_next += r.exponential(1 / 200.0)
+            while time.perf_counter() < t_next and not stop_up.is_set():
+                time.sleep(0.0005)
+            g = ups[i % len(ups)]
+            i += 1
+            try:
+                gid = srv.upload(*g)
+            except Exception:
+                continue  # not admitted: the stream moves on
+            now = time.perf_counter()
+            with live_lock:
+                live.append(gid)
+            held.append((now, gid))
+            while held and now - held[0][0] > 2.0:
+                _, old = held.pop(0)
+                with live_lock:
+                    live.remove(old)
+                srv.release(old)
+        for _, gid in held:
+            with live_lock:
+                if gid in live:
+                    live.remove(gid)
+            srv.release(gid)
+
+    upt = threading.Thread(target=uploader, daemon=True)
+    upt.start()
+    while True:
+        with live_lock:
+            if len(live) >= 50:
+                break
+        time.sleep(0.01)
+
+    def drive(rate, count, seed):
+        """Open-loop Poisson arrivals at `rate`; returns per-query infos."""
+        rng = np.random.default_rng(seed)
+        kind, a, b = serve_queries(n, rng, count)
+        gaps = rng.exponential(1.0 / rate, count)
+        infos, tickets = [], []
+        t0 = time.perf_counter()
+        t_next = t0
+        for i in range(count):
+            t_next += gaps[i]
+            while time.perf_counter() < t_next:
+                pass
+            if kind[i] == 0:
+                tickets.append(srv.shortest_path(int(a[i]), int(b[i])))
+            elif kind[i] == 1:
+                tickets.append(srv.hop(int(a[i]), 2))
+            else:
+                with live_lock:
+                    gid = live[int(b[i]) % len(live)]
+                tickets.append(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
+        offered = count / (time.perf_counter() - t0)
+        for t in tickets:
+            infos.append(srv.result(t, timeout_s=600))
+        return infos, offered, kind
+
+    def summarize(infos, kind):
+        lat = np.array([x.latency_us for x in infos]) / 1e3
+        t_first = min(x.submit_us for x in infos)
+        t_last = max(x.done_us for x in infos)
+        out = {"completed_qps": len(infos) / ((t_last - t_first) * 1e-6),
+               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+               "errors": int(sum(1 for x in infos if x.status != 0))}
+        for k, name in ((0, "shortest_path"), (1, "hop2"), (2, "pagerank")):
+            sel = lat[kind == k]
+            if sel.size:
+                out[name] = {"p50_ms": float(np.percentile(sel, 50)), "p99_ms": float(np.percentile(sel, 99))}
+        return out
+
+    drive(2000, 2000, 1)  # warm-up
+    launches0 = L.ursa_gpu_launch_count()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    sweep = []
+    total_q = 0
+    for j, rate in enumerate(SERVE_RATES):
+        count = int(min(max(rate * 3, 3000), 60000))
+        infos, offered, kind = drive(rate, count, 100 + j)
+        total_q += count
+        row = {"rate_qps": rate, "offered_qps": offered, "queries": count}
+        row.update(summarize(infos, kind))
+        sweep.append(row)
+    # closed loop: everything submitted at once (maximum sustained throughput)
+    infos, offered, kind = drive(1e9, 60000, 999)
+    total_q += 60000
+    closed = summarize(infos, kind)
+    clocks = sampler.stop() if sampler else None
+    launches = L.ursa_gpu_launch_count() - launches0
+    stats = srv.stats()
+
+    # the plain path: one query per C-ABI call, 4 host threads, closed loop
+    plain_topos = {}
+    rng = np.random.default_rng(4242)
+    kind, a, b = serve_queries(n, rng, 2000)
+    pr_params = PageRankParams(DAMPING, MAX_ITER, TOL)
+    for i in range(len(ups)):
+        if len(plain_topos) >= 64:
+            break
+        plain_topos[i] = Topology.build(*ups[i])
+    keys = list(plain_topos)
+    lat = np.zeros(len(kind))
+
+    def plain_one(i):
+        t0 = time.perf_counter()
+        if kind[i] == 0:
+            algo.shortest_path(topo, int(a[i]), int(b[i]))
+        elif kind[i] == 1:
+            algo.k_hop(topo, [int(a[i])], 2)
+        else:
+            algo.pagerank(plain_topos[keys[int(b[i]) % len(keys)]], pr_params)
+        lat[i] = time.perf_counter() - t0
+
+    import concurrent.futures as cf
+
+    with cf.ThreadPoolExecutor(4) as ex:
+        list(ex.map(plain_one, range(200)))  # warm-up (plans, pools)
+        t0 = time.perf_counter()
+        list(ex.map(plain_one, range(len(kind))))
+        plain_s = time.perf_counter() - t0
+    plain = {"completed_qps": len(kind) / plain_s, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+             "p99_ms": float(np.percentile(lat, 99) * 1e3), "queries": int(len(kind)), "threads": 4,
+             "note": "closed loop; latency is the per-call service time (no queueing)"}
+    stop_up.set()
+    upt.join(timeout=30)
+    srv.close()
+
+    if rank == 0:
+        best = max(sweep, key=lambda r: r["completed_qps"])
+        line = {
+            "metric": "serve_queries_per_s",
+            "value": closed["completed_qps"],
+            "unit": "queries/s",
+            "n_gpus": world,
+            "steps": len(SERVE_RATES) + 1,
+            "warmup": 1,
+            "ms_per_step": None,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u32 ids; f32-compensated pagerank SpMV, f64 ranks",
+            "data": "synthetic",
+            "config": {"workload": SERVE_WORKLOAD, "resident_nodes": n, "resident_edges": m,
+                       "uploads": "Poisson 200/s, 2 s lifetime, rmat_batch sizes",
+                       "mix": {"shortest_path": 0.5, "hop2": 0.3, "pagerank": 0.2},
+                       "lanes": {"shortest_path": [4, 16], "hop": [4, 16], "pagerank": [2, 32]}},
+            "closed_loop": closed,
+            "sweep": sweep,
+            "best_open_loop": {"rate_qps": best["rate_qps"], "completed_qps": best["completed_qps"]},
+            "plain_one_query_per_launch": plain,
+            "speedup_vs_plain": closed["completed_qps"] / plain["completed_qps"],
+            "e2e": {"value": closed["completed_qps"], "unit": "queries/s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None,
+                    "note": "every query is submitted from and returned to host memory through the C ABI"},
+            "server_stats": stats,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_batch(args, rank, world):
     import torch
 
@@ -458,7 +681,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch"])
+    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
@@ -475,6 +698,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args, rank, world)
+        return
+    if args.workload == "serve":
+        run_serve(args, rank, world)
         return
 
     import torch

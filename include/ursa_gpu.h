@@ -42,7 +42,8 @@ enum {
   URSA_GPU_ECUDA = 3,    /* CUDA runtime error */
   URSA_GPU_ETIMEOUT = 4, /* a bounded device-side wait expired */
   URSA_GPU_ETRUNC = 5,   /* caller buffer too small; required size reported */
-  URSA_GPU_ENODEV = 6    /* no usable CUDA device */
+  URSA_GPU_ENODEV = 6,   /* no usable CUDA device */
+  URSA_GPU_ECANCELED = 7 /* a served query was cancelled */
 };
 
 typedef struct ursa_gpu_topo ursa_gpu_topo;
@@ -294,6 +295,101 @@ int ursa_gpu_batch_results(ursa_gpu_batch *b, double *pagerank, uint32_t *compon
 /* Device addresses of the same result arrays (valid until ursa_gpu_batch_free). */
 int ursa_gpu_batch_device_results(ursa_gpu_batch *b, const double **pagerank,
                                   const uint32_t **components, const uint32_t **triangles);
+
+/* ------------------------------------------------------------------------
+ * Serving loop.
+ *
+ * The reference answers each query with one kernel call through its plan
+ * layer: shortest_path (algo/bfs.rs:48-102, via ursa-plan/src/result.rs:216),
+ * k_hop (algo/hop.rs:52-130, via result.rs:180) and pagerank
+ * (algo/pagerank.rs:98-124, via result.rs:82-140).  A server keeps a resident
+ * topology (shortest_path and hop queries) and uploaded small graphs
+ * (pagerank queries) on the device and runs submitted queries with
+ * continuous batching: each lane (a stream with preallocated slots, one
+ * query type) launches one kernel for up to `slots` pending queries, lanes
+ * run concurrently, and a lane is refilled as soon as its launch finishes.
+ * Results do not depend on the other queries of a launch:
+ *  - shortest_path: a shortest path over out-edges (bidirectional BFS; hop
+ *    count equal to the reference's; on ties the path may differ from the
+ *    reference's serial-order choice), -1 length when there is none;
+ *  - hop: the nodes k_hop(&[seed], k, Out) pairs with the seed, in the
+ *    reference's emission order;
+ *  - pagerank: the batch kernel's ranks of the uploaded graph.
+ * ---------------------------------------------------------------------- */
+typedef struct ursa_gpu_server ursa_gpu_server;
+
+enum {
+  URSA_GPU_QUERY_SHORTEST_PATH = 1,
+  URSA_GPU_QUERY_HOP = 2,
+  URSA_GPU_QUERY_PAGERANK = 3
+};
+
+typedef struct {
+  uint32_t path_lanes, path_slots; /* shortest_path: lanes and queries per launch */
+  uint32_t hop_lanes, hop_slots;
+  uint32_t pr_lanes, pr_slots;
+  uint64_t pr_max_nodes;           /* largest uploaded graph, in nodes */
+  uint64_t hbm_reserve_bytes;      /* free HBM an upload must leave */
+  uint64_t upload_budget_bytes;    /* device bytes of live uploads (0 = no cap) */
+} ursa_gpu_server_config;
+
+typedef struct {
+  uint32_t type;     /* URSA_GPU_QUERY_* */
+  uint32_t graph;    /* pagerank: the uploaded graph's id */
+  uint32_t source;   /* shortest_path source, hop seed */
+  uint32_t target;   /* shortest_path target */
+  uint32_t k;        /* hop depth */
+  ursa_gpu_pagerank_params pr;
+} ursa_gpu_query;
+
+typedef struct {
+  int32_t status;     /* URSA_GPU_OK, URSA_GPU_ECANCELED, ... */
+  uint32_t type;
+  int64_t result_len; /* path nodes (-1 = no path), reached nodes, or ranks */
+  uint32_t iterations;
+  double last_delta;
+  uint64_t edges;     /* edges the query scanned */
+  double submit_us, launch_us, done_us; /* host steady clock */
+} ursa_gpu_query_info;
+
+typedef struct {
+  uint64_t submitted, completed, launches;
+  uint64_t uploads_admitted, uploads_rejected, uploads_live, upload_bytes, pending;
+} ursa_gpu_server_stats;
+
+/* Creates a server over `resident` (may be NULL when no path/hop lanes are
+ * configured; the caller keeps it alive until the server is destroyed).
+ * Every slot's scratch is allocated here (shortest_path 32 B and hop 20 B
+ * per resident node per slot). */
+int ursa_gpu_server_create(ursa_gpu_topo *resident, const ursa_gpu_server_config *cfg,
+                           ursa_gpu_server **out);
+/* Stops the scheduler (queries in flight finish; pending ones are dropped)
+ * and frees everything the server owns, uploads included. */
+void ursa_gpu_server_destroy(ursa_gpu_server *s);
+/* Uploads a graph (Topology::build arguments) for pagerank queries.
+ * Admission by free HBM: URSA_GPU_ENOMEM when the build would leave less
+ * than hbm_reserve_bytes free or exceed upload_budget_bytes. */
+int ursa_gpu_server_upload(ursa_gpu_server *s, uint64_t n_nodes, const uint32_t *src,
+                           const uint32_t *dst, uint64_t n_edges, uint32_t *graph_id);
+/* Frees an upload once the queries that use it have finished. */
+int ursa_gpu_server_release(ursa_gpu_server *s, uint32_t graph_id);
+/* Queues a query; *ticket identifies it. */
+int ursa_gpu_server_submit(ursa_gpu_server *s, const ursa_gpu_query *q, uint64_t *ticket);
+/* Cancels a query: a queued one completes at once with URSA_GPU_ECANCELED,
+ * a running shortest_path / hop stops at its next BFS level. */
+int ursa_gpu_server_cancel(ursa_gpu_server *s, uint64_t ticket);
+/* Waits up to timeout_us (0 = just look) for a query; URSA_GPU_ETIMEOUT if
+ * it has not completed.  info may be NULL. */
+int ursa_gpu_server_wait(ursa_gpu_server *s, uint64_t ticket, uint64_t timeout_us,
+                         ursa_gpu_query_info *info);
+/* Tickets completed since the last poll (up to cap). */
+int ursa_gpu_server_poll(ursa_gpu_server *s, uint64_t *tickets, uint64_t cap, uint64_t *n_out);
+/* Hands over a completed query's result and forgets the ticket: u32 nodes
+ * (path, hop) or f64 ranks (pagerank), info.result_len elements (0 for no
+ * path); URSA_GPU_ETRUNC if cap_elems is too small. */
+int ursa_gpu_server_result(ursa_gpu_server *s, uint64_t ticket, ursa_gpu_query_info *info,
+                           void *out, uint64_t cap_elems);
+int ursa_gpu_server_get_stats(ursa_gpu_server *s, ursa_gpu_server_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -12,7 +12,7 @@ import os
 PKG = os.path.dirname(os.path.abspath(__file__))
 GPU_SO = os.path.join(PKG, "libursa_gpu.so")
 
-OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ETRUNC, ENODEV = range(7)
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ETRUNC, ENODEV, ECANCELED = range(8)
 _STATUS = {
     EINVAL: "EINVAL",
     ENOMEM: "ENOMEM",
@@ -20,6 +20,7 @@ _STATUS = {
     ETIMEOUT: "ETIMEOUT",
     ETRUNC: "ETRUNC",
     ENODEV: "ENODEV",
+    ECANCELED: "ECANCELED",
 }
 
 
@@ -65,6 +66,52 @@ class BatchConfig(C.Structure):
 
 
 BATCH_PAGERANK, BATCH_COMPONENTS, BATCH_TRIANGLES = 1, 2, 4
+
+QUERY_SHORTEST_PATH, QUERY_HOP, QUERY_PAGERANK = 1, 2, 3
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("path_lanes", C.c_uint32),
+        ("path_slots", C.c_uint32),
+        ("hop_lanes", C.c_uint32),
+        ("hop_slots", C.c_uint32),
+        ("pr_lanes", C.c_uint32),
+        ("pr_slots", C.c_uint32),
+        ("pr_max_nodes", C.c_uint64),
+        ("hbm_reserve_bytes", C.c_uint64),
+        ("upload_budget_bytes", C.c_uint64),
+    ]
+
+
+class Query(C.Structure):
+    _fields_ = [
+        ("type", C.c_uint32),
+        ("graph", C.c_uint32),
+        ("source", C.c_uint32),
+        ("target", C.c_uint32),
+        ("k", C.c_uint32),
+        ("pr", PageRankParams),
+    ]
+
+
+class QueryInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("type", C.c_uint32),
+        ("result_len", C.c_int64),
+        ("iterations", C.c_uint32),
+        ("last_delta", C.c_double),
+        ("edges", C.c_uint64),
+        ("submit_us", C.c_double),
+        ("launch_us", C.c_double),
+        ("done_us", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "launches", "uploads_admitted",
+                                           "uploads_rejected", "uploads_live", "upload_bytes", "pending")]
 
 # Every exported symbol with its (restype, argtypes).
 P, u32, u64, i32, i64, f64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_int64, C.c_double
@@ -122,6 +169,16 @@ SIGNATURES = {
     "ursa_gpu_batch_get_config": (i32, [P, C.POINTER(BatchConfig)]),
     "ursa_gpu_batch_results": (i32, [P, P, P, P, P, P]),
     "ursa_gpu_batch_device_results": (i32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "ursa_gpu_server_create": (i32, [P, C.POINTER(ServerConfig), C.POINTER(P)]),
+    "ursa_gpu_server_destroy": (None, [P]),
+    "ursa_gpu_server_upload": (i32, [P, u64, P, P, u64, C.POINTER(u32)]),
+    "ursa_gpu_server_release": (i32, [P, u32]),
+    "ursa_gpu_server_submit": (i32, [P, C.POINTER(Query), C.POINTER(u64)]),
+    "ursa_gpu_server_cancel": (i32, [P, u64]),
+    "ursa_gpu_server_wait": (i32, [P, u64, u64, C.POINTER(QueryInfo)]),
+    "ursa_gpu_server_poll": (i32, [P, P, u64, C.POINTER(u64)]),
+    "ursa_gpu_server_result": (i32, [P, u64, C.POINTER(QueryInfo), P, u64]),
+    "ursa_gpu_server_get_stats": (i32, [P, C.POINTER(ServerStats)]),
 }
 
 _lib = None

@@ -35,6 +35,7 @@
 
 #include "frontier.cuh"
 #include "primitives.cuh"
+#include "batch.cuh"
 #include "unionfind.cuh"
 
 namespace ug {
@@ -42,45 +43,11 @@ namespace ug {
 namespace {
 
 constexpr int kBkMaxBuckets = 3;
-constexpr uint32_t kBkWhatPr = 1, kBkWhatCc = 2, kBkWhatTc = 4;
 // Shared-memory budget of one CTA for per-node state (f32 shares, u32
 // parents or counts), leaving room for the static reduction area.
 constexpr uint32_t kBkSmemBytesMax = 224u * 1024u;
 
 typedef unsigned __int128 u128;
-
-// One graph of a batch.  Row pointers are offset to the graph's first row;
-// ids stored in in_src / o_tgt are `id_base` + local id.
-struct __align__(16) GraphDesc {
-  const uint32_t* in_off;   // n + 1 (values index in_src)
-  const uint32_t* in_src;
-  const uint32_t* out_off;  // n + 1 (out-degree only)
-  const uint32_t* o_off;    // n + 1 (values index o_tgt)
-  const uint32_t* o_tgt;    // oriented undirected lists, ascending ids
-  const uint32_t* rows;     // local rows grouped by degree class
-  double* rank;             // n (pagerank result, updated in place)
-  float* x0;                // n (global share row: staging or shares)
-  float* x1;                // n
-  uint32_t* cc;             // n
-  uint32_t* tri;            // n
-  uint32_t cls[8];          // class c rows: rows[cls[c] .. cls[c+1]), cls[6] = n
-  uint32_t n;
-  uint32_t id_base;
-  uint32_t pad[2];
-};
-
-struct BucketArgs {
-  const GraphDesc* desc;
-  const uint32_t* work;  // descriptor indices, largest graph first
-  uint32_t n_work;
-  uint32_t* next;        // work counter (zeroed before the launch)
-  uint32_t cap;          // nodes whose state fits in the CTA's shared memory
-  uint32_t what;
-  uint32_t max_iter;
-  double damping, tol;
-  uint32_t* iters;       // per descriptor
-  double* delta;         // per descriptor
-};
 
 struct BkShared {
   GraphDesc g;
@@ -589,6 +556,7 @@ struct ursa_gpu_batch {
   OrientedCsr orient;
   DevArray<uint32_t> rows;
   DevArray<GraphDesc> desc;
+  std::vector<GraphDesc> h_desc;  // host copy of desc
   DevArray<double> rank, delta;
   DevArray<float> x;
   DevArray<uint32_t> cc, tri, iters;
@@ -855,6 +823,17 @@ void batch_launch(ursa_gpu_batch* b, const ursa_gpu_pagerank_params& p, uint32_t
 }
 
 }  // namespace
+
+void* batch_kernel_for(uint32_t threads) { return batch_fn_for(threads); }
+
+int batch_kernel_resident(uint32_t threads, size_t smem, int device) {
+  return resident_ctas(batch_fn_for(threads), threads, smem, device);
+}
+
+const GraphDesc* batch_host_desc(const ursa_gpu_batch* b, uint64_t g) {
+  return b && g < b->h_desc.size() ? &b->h_desc[g] : nullptr;
+}
+
 }  // namespace ug
 
 extern "C" {
@@ -982,6 +961,7 @@ int ursa_gpu_batch_build(uint64_t n_graphs, const uint64_t* node_counts,
       d.cls[6] = d.cls[7] = d.n;
       d.id_base = base;
     }
+    b->h_desc = desc;
     b->desc.alloc(n_graphs ? n_graphs : 1, s);
     if (n_graphs)
       UG_CUDA(cudaMemcpyAsync(b->desc.get(), desc.data(), n_graphs * sizeof(GraphDesc),
