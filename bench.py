@@ -449,6 +449,11 @@ def run_serve(args, rank, world):
     launches = L.ursa_gpu_launch_count() - launches0
     stats = srv.stats()
 
+    # the server (and its uploads) go before the plain path is timed
+    stop_up.set()
+    upt.join(timeout=30)
+    srv.close()
+
     # the plain path: one query per C-ABI call, 4 host threads, closed loop
     plain_topos = {}
     rng = np.random.default_rng(4242)
@@ -481,9 +486,6 @@ def run_serve(args, rank, world):
     plain = {"completed_qps": len(kind) / plain_s, "p50_ms": float(np.percentile(lat, 50) * 1e3),
              "p99_ms": float(np.percentile(lat, 99) * 1e3), "queries": int(len(kind)), "threads": 4,
              "note": "closed loop; latency is the per-call service time (no queueing)"}
-    stop_up.set()
-    upt.join(timeout=30)
-    srv.close()
 
     if rank == 0:
         best = max(sweep, key=lambda r: r["completed_qps"])

@@ -376,13 +376,19 @@ __device__ HopOut hop_query(const HopArgs& A, const HopQuery q, const HopSlot& S
 }
 
 // ------------------------------------------------------- persistent lanes
-// A slot's mailbox lives in pinned host memory mapped into the device.  The
-// host writes the query fields, then bumps seq_in; the slot's CTA answers by
-// writing the result fields, then setting seq_out = seq_in.
-struct alignas(64) Mailbox {
-  uint32_t seq_in;
-  uint32_t cancel;
+// A slot's query lives in DEVICE memory (the CTA polls only its own GPU's
+// memory): the host writes the fields with one async copy and then seq_in
+// with a second copy on the same stream.  The CTA answers into pinned host
+// memory mapped into the device (posted writes): the result fields, then
+// seq_out = seq_in, which the host polls locally.
+struct alignas(32) DevMail {
   uint32_t a, b, k, base;  // source / seed, target, hop depth, stamp base
+  uint32_t cancel;
+  uint32_t pad[2];
+  uint32_t seq_in;
+};
+
+struct alignas(32) HostMail {
   uint32_t seq_out;
   int32_t len, status;
   uint32_t pad;
@@ -392,12 +398,12 @@ struct alignas(64) Mailbox {
 struct LaneCtl {
   uint32_t stop;       // host: the lane's CTAs return
   uint32_t heartbeat;  // host: bumped by the scheduler while it runs
-  uint32_t pad[14];
 };
 
 struct LaneArgs {
-  Mailbox* mail;        // slots (device view of the mapped mailboxes)
-  const LaneCtl* ctl;   // device view
+  const DevMail* mail;  // slots (device memory)
+  HostMail* res;        // slots (mapped host memory)
+  const LaneCtl* ctl;   // device memory
   uint32_t* paths;      // shortest_path: slots * kPathCap (mapped host memory)
   PathArgs pa;
   const PathSlot* pslots;
@@ -423,19 +429,21 @@ __global__ void __launch_bounds__(kSvThreads) lane_k(LaneArgs A) {
   __shared__ HopShared hsh;
   __shared__ uint32_t cmd[6];  // stop, seq, a, b, k, base
   const uint32_t slot = blockIdx.x;
-  Mailbox* mb = A.mail + slot;
+  const DevMail* mb = A.mail + slot;
+  HostMail* hr = A.res + slot;
+  uint32_t done_seq = vload(&hr->seq_out);
   while (true) {
     if (threadIdx.x == 0) {
       uint32_t hb_last = vload(&A.ctl->heartbeat);
       uint64_t t_hb = global_ns(), t_idle = t_hb;
       uint32_t stop = 0, si = 0;
       while (true) {
-        si = vload(&mb->seq_in);
         if (vload(&A.ctl->stop)) {
           stop = 1;
           break;
         }
-        if (si != vload(&mb->seq_out)) break;
+        si = vload(&mb->seq_in);
+        if (si != done_seq) break;
         const uint64_t now = global_ns();
         const uint32_t hb = vload(&A.ctl->heartbeat);
         if (hb != hb_last) {
@@ -446,9 +454,9 @@ __global__ void __launch_bounds__(kSvThreads) lane_k(LaneArgs A) {
           stop = 1;
           break;
         }
-        __nanosleep(1000);
+        __nanosleep(500);
       }
-      __threadfence_system();  // the query fields are read after seq_in
+      __threadfence();  // the query fields are read after seq_in
       cmd[0] = stop;
       cmd[1] = si;
       cmd[2] = vload(&mb->a);
@@ -474,13 +482,13 @@ __global__ void __launch_bounds__(kSvThreads) lane_k(LaneArgs A) {
       edges = o.edges;
     }
     __syncthreads();
+    done_seq = cmd[1];
     if (threadIdx.x == 0) {
-      __threadfence();  // the slot's device buffers are complete
-      *(volatile int32_t*)&mb->len = len;
-      *(volatile int32_t*)&mb->status = status;
-      *(volatile uint64_t*)&mb->edges = edges;
-      __threadfence_system();  // results (and the mapped path) before seq_out
-      *(volatile uint32_t*)&mb->seq_out = cmd[1];
+      *(volatile int32_t*)&hr->len = len;
+      *(volatile int32_t*)&hr->status = status;
+      *(volatile uint64_t*)&hr->edges = edges;
+      __threadfence_system();  // device buffers, results and the mapped path before seq_out
+      *(volatile uint32_t*)&hr->seq_out = done_seq;
     }
     __syncthreads();
   }
@@ -529,10 +537,12 @@ struct Lane {
   bool stopping = false;          // stop raised, kernel not yet returned
   double last_use = 0.0;          // host clock of the last post or harvest
   // path / hop: persistent slots
-  Mailbox* mail = nullptr;        // mapped, host view
-  Mailbox* d_mail = nullptr;      // device view
-  LaneCtl* ctl = nullptr;
-  LaneCtl* d_ctl = nullptr;
+  DevArray<DevMail> d_mail;       // queries (device)
+  DevMail* h_stage = nullptr;     // pinned staging of the queries
+  DevArray<LaneCtl> d_ctl;        // stop / heartbeat (device)
+  LaneCtl* h_ctl = nullptr;       // pinned staging of the control words
+  HostMail* res = nullptr;        // mapped, host view
+  HostMail* d_res = nullptr;      // device view
   uint32_t* paths = nullptr;      // mapped, host view
   uint32_t* d_paths = nullptr;
   std::vector<std::shared_ptr<Request>> slot_req;  // request in each slot (null = free)
@@ -572,6 +582,7 @@ struct ursa_gpu_server {
   ursa_gpu_server_stats stats{};
   std::thread sched;
   std::atomic<bool> stop{false};
+  double last_heartbeat = 0.0;
   std::string fatal;  // a CUDA failure in the scheduler ends the server
 };
 
@@ -586,12 +597,24 @@ void free_pinned(void* p) {
   if (p) cudaFreeHost(p);
 }
 
+// Raises the lane's stop word (its CTAs return within a poll).
+void lane_raise_stop(Lane& L) {
+  if (!L.h_ctl) return;
+  L.h_ctl->stop = 1;
+  cudaMemcpyAsync(&L.d_ctl.get()->stop, &L.h_ctl->stop, 4, cudaMemcpyHostToDevice, L.copy);
+  cudaStreamSynchronize(L.copy);
+}
+
+// Frees a lane; every lane's stop must have been raised first (freeing
+// pinned memory synchronises the whole device).
 void lane_destroy(Lane& L) {
-  if (L.ctl) *(volatile uint32_t*)&L.ctl->stop = 1;
   if (L.stream) cudaStreamSynchronize(L.stream);
   if (L.copy) cudaStreamSynchronize(L.copy);
-  free_pinned(L.mail);
-  free_pinned(L.ctl);
+  L.d_mail.release();
+  L.d_ctl.release();
+  free_pinned(L.h_stage);
+  free_pinned(L.h_ctl);
+  free_pinned(L.res);
   free_pinned(L.paths);
   free_pinned(L.h_iters);
   free_pinned(L.h_delta);
@@ -619,8 +642,15 @@ void lane_create(ursa_gpu_server* S, Lane& L, LaneKind kind, uint32_t slots) {
   UG_CUDA(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
   cudaStream_t s = L.stream;
   if (kind == kLanePath || kind == kLaneHop) {
-    L.mail = mapped_alloc<Mailbox>(slots, &L.d_mail);
-    L.ctl = mapped_alloc<LaneCtl>(1, &L.d_ctl);
+    L.d_mail.alloc(slots, s);
+    UG_CUDA(cudaMemsetAsync(L.d_mail.get(), 0, slots * sizeof(DevMail), s));
+    UG_CUDA(cudaMallocHost((void**)&L.h_stage, slots * sizeof(DevMail)));
+    std::memset((void*)L.h_stage, 0, slots * sizeof(DevMail));
+    L.d_ctl.alloc(1, s);
+    UG_CUDA(cudaMemsetAsync(L.d_ctl.get(), 0, sizeof(LaneCtl), s));
+    UG_CUDA(cudaMallocHost((void**)&L.h_ctl, sizeof(LaneCtl)));
+    std::memset((void*)L.h_ctl, 0, sizeof(LaneCtl));
+    L.res = mapped_alloc<HostMail>(slots, &L.d_res);
     L.slot_req.assign(slots, nullptr);
     L.seq.assign(slots, 0);
     L.base.assign(slots, kStampStride);
@@ -676,12 +706,16 @@ void lane_create(ursa_gpu_server* S, Lane& L, LaneKind kind, uint32_t slots) {
 
 // (Re)launches a path / hop lane's persistent kernel.
 void lane_start(ursa_gpu_server* S, Lane& L) {
-  *(volatile uint32_t*)&L.ctl->stop = 0;  // the previous kernel has returned
+  L.h_ctl->stop = 0;  // the previous kernel has returned
+  UG_CUDA(cudaMemcpyAsync(&L.d_ctl.get()->stop, &L.h_ctl->stop, 4, cudaMemcpyHostToDevice, L.copy));
+  UG_CUDA(cudaEventRecord(L.done, L.copy));
+  UG_CUDA(cudaStreamWaitEvent(L.stream, L.done, 0));  // the launch sees stop = 0
   L.stopping = false;
   L.last_use = now_us();
   LaneArgs a{};
-  a.mail = L.d_mail;
-  a.ctl = L.d_ctl;
+  a.mail = L.d_mail.get();
+  a.res = L.d_res;
+  a.ctl = L.d_ctl.get();
   a.paths = L.d_paths;
   const TopoImpl* t = S->topo;
   a.pa = PathArgs{t->out.off.get(), t->out.tgt.get(), t->in.off.get(), t->in.tgt.get(), t->n};
@@ -715,15 +749,17 @@ uint32_t take_base(Lane& L, uint32_t slot, uint64_t n) {
 }
 
 void post(ursa_gpu_server* S, Lane& L, uint32_t slot, const std::shared_ptr<Request>& r) {
-  Mailbox* mb = L.mail + slot;
-  mb->a = r->q.source;
-  mb->b = r->q.target;
-  mb->k = r->q.k;
-  mb->base = take_base(L, slot, S->topo->n);
-  mb->cancel = r->cancel ? 1u : 0u;
-  std::atomic_thread_fence(std::memory_order_release);
-  L.seq[slot]++;
-  *(volatile uint32_t*)&mb->seq_in = L.seq[slot];
+  DevMail* st = L.h_stage + slot;  // untouched until the slot completes
+  st->a = r->q.source;
+  st->b = r->q.target;
+  st->k = r->q.k;
+  st->base = take_base(L, slot, S->topo->n);
+  st->cancel = r->cancel ? 1u : 0u;
+  st->seq_in = ++L.seq[slot];
+  DevMail* d = L.d_mail.get() + slot;
+  // fields first, then the sequence number: copies on one stream run in order
+  UG_CUDA(cudaMemcpyAsync(d, st, offsetof(DevMail, seq_in), cudaMemcpyHostToDevice, L.copy));
+  UG_CUDA(cudaMemcpyAsync(&d->seq_in, &st->seq_in, 4, cudaMemcpyHostToDevice, L.copy));
   L.slot_req[slot] = r;
   r->info.launch_us = now_us();
   L.last_use = r->info.launch_us;
@@ -733,7 +769,7 @@ void post(ursa_gpu_server* S, Lane& L, uint32_t slot, const std::shared_ptr<Requ
 // taken until this returns).
 void slot_harvest(Lane& L, uint32_t slot, Request& r) {
   std::atomic_thread_fence(std::memory_order_acquire);
-  const Mailbox* mb = L.mail + slot;
+  const HostMail* mb = L.res + slot;
   r.info.status = *(const volatile int32_t*)&mb->status;
   r.info.edges = *(const volatile uint64_t*)&mb->edges;
   const int32_t len = *(const volatile int32_t*)&mb->len;
@@ -839,8 +875,16 @@ void sched_loop(ursa_gpu_server* S) {
   while (!S->stop.load()) {
     bool progressed = false;
     try {
-      for (auto& lp : S->lanes)
-        if (lp->ctl) *(volatile uint32_t*)&lp->ctl->heartbeat += 1;
+      const double t_now = now_us();
+      if (t_now - S->last_heartbeat > 1000.0) {  // about once a millisecond
+        S->last_heartbeat = t_now;
+        for (auto& lp : S->lanes)
+          if (lp->h_ctl && lp->running) {
+            lp->h_ctl->heartbeat++;
+            UG_CUDA(cudaMemcpyAsync(&lp->d_ctl.get()->heartbeat, &lp->h_ctl->heartbeat, 4,
+                                    cudaMemcpyHostToDevice, lp->copy));
+          }
+      }
       for (auto& lp : S->lanes) {
         Lane& L = *lp;
         if (L.kind == kLanePr) {
@@ -886,7 +930,7 @@ void sched_loop(ursa_gpu_server* S) {
         for (uint32_t i = 0; i < L.slots; i++) {
           auto r = L.slot_req[i];
           if (!r) continue;
-          if (*(const volatile uint32_t*)&L.mail[i].seq_out != L.seq[i]) continue;
+          if (*(const volatile uint32_t*)&L.res[i].seq_out != L.seq[i]) continue;
           lk.unlock();
           slot_harvest(L, i, *r);
           lk.lock();
@@ -906,7 +950,8 @@ void sched_loop(ursa_gpu_server* S) {
         for (uint32_t i = 0; i < L.slots; i++) waiting |= L.slot_req[i] != nullptr;
         if (waiting && !L.running) lane_start(S, L);
         if (!waiting && L.running && !L.stopping && now_us() - L.last_use > kLaneIdleStopUs) {
-          *(volatile uint32_t*)&L.ctl->stop = 1;  // idle lane: give its SMs back
+          L.h_ctl->stop = 1;  // idle lane: give its SMs back
+          UG_CUDA(cudaMemcpyAsync(&L.d_ctl.get()->stop, &L.h_ctl->stop, 4, cudaMemcpyHostToDevice, L.copy));
           L.stopping = true;
         }
         progressed |= posted;
@@ -996,6 +1041,7 @@ int ursa_gpu_server_create(ursa_gpu_topo* resident, const ursa_gpu_server_config
       add(kLaneHop, cfg->hop_lanes, cfg->hop_slots);
       add(kLanePr, cfg->pr_lanes, cfg->pr_slots);
     } catch (...) {
+      for (auto& l : S->lanes) lane_raise_stop(*l);
       for (auto& l : S->lanes) lane_destroy(*l);
       throw;
     }
@@ -1015,6 +1061,7 @@ void ursa_gpu_server_destroy(ursa_gpu_server* S) {
   S->cv_sched.notify_all();
   if (S->sched.joinable()) S->sched.join();
   cudaSetDevice(S->device);
+  for (auto& l : S->lanes) lane_raise_stop(*l);
   for (auto& l : S->lanes) lane_destroy(*l);
   for (auto& kv : S->uploads) ursa_gpu_batch_free(kv.second->batch);
   delete S;
@@ -1153,7 +1200,11 @@ int ursa_gpu_server_cancel(ursa_gpu_server* S, uint64_t ticket) {
     for (auto& lp : S->lanes) {
       Lane& L = *lp;
       for (size_t i = 0; i < L.slot_req.size(); i++)
-        if (L.slot_req[i] == r) *(volatile uint32_t*)&L.mail[i].cancel = 1u;
+        if (L.slot_req[i] == r) {
+          L.h_stage[i].cancel = 1u;
+          UG_CUDA(cudaMemcpyAsync(&L.d_mail.get()[i].cancel, &L.h_stage[i].cancel, 4,
+                                  cudaMemcpyHostToDevice, L.copy));
+        }
     }
   });
 }
