@@ -56,6 +56,7 @@ struct PrClassTable {
 
 struct PrPlan {
   PrClassTable cls{};
+  uint32_t iso_lo = 0;  // rows [iso_lo, n) are isolated: rank follows in closed form
   uint32_t n_units = 0, n_hub = 0, n_chunks = 0;
   DevArray<uint2> hub_unit;            // per hub chunk: {hub index, chunk}
   DevArray<uint32_t> hub_first, hub_nch;
@@ -76,10 +77,20 @@ uint64_t pr_plan_bytes(const PrPlan* p) {
 namespace {
 
 // ------------------------------------------------------------ plan kernels
-__global__ void neg_indeg_k(const uint32_t* __restrict__ off, uint64_t n, uint32_t* __restrict__ key) {
+// Relabel key, ascending = execution order: in-degree high to low; among
+// in-degree-0 nodes, sources (out-degree > 0) before isolated nodes, which
+// end the order (their ranks follow in closed form).
+__global__ void exec_order_key_k(const uint32_t* __restrict__ in_off,
+                                 const uint32_t* __restrict__ out_off, uint64_t n,
+                                 uint32_t* __restrict__ key) {
   for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x)
-    key[u] = ~(off[u + 1] - off[u]);  // ascending ~deg == descending degree
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t din = in_off[u + 1] - in_off[u];
+    const uint64_t dout = out_off[u + 1] - out_off[u];
+    uint64_t r = din ? 2 * din : (dout ? 1 : 0);
+    if (r > 0xFFFFFFFEull) r = 0xFFFFFFFEull;
+    key[u] = ~(uint32_t)r;
+  }
 }
 
 __global__ void relabel_maps_k(const uint32_t* __restrict__ old_of_new, uint64_t n,
@@ -113,9 +124,10 @@ __global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n,
 }
 
 // Class boundaries over the non-increasing degree sequence: bounds[t] =
-// number of rows with degree > thr[t].
-__global__ void class_bounds_k(const uint32_t* __restrict__ deg, uint64_t n,
-                               uint32_t* __restrict__ bounds) {
+// number of rows with degree > thr[t]; bounds[kClasses - 1] = first isolated
+// row (in- and out-degree 0; they end the execution order).
+__global__ void class_bounds_k(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ outdeg,
+                               uint64_t n, uint32_t* __restrict__ bounds) {
   const uint32_t thr[kClasses - 1] = {kHubDeg, 64u, 32u, 16u, 8u, 4u};
   for (int t = 0; t < kClasses - 1; t++) {
     uint64_t lo = 0, hi = n;  // first index with deg <= thr
@@ -128,6 +140,15 @@ __global__ void class_bounds_k(const uint32_t* __restrict__ deg, uint64_t n,
     }
     bounds[t] = (uint32_t)lo;
   }
+  uint64_t lo = 0, hi = n;  // first isolated row
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (deg[mid] != 0 || outdeg[mid] != 0)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  bounds[kClasses - 1] = (uint32_t)lo;
 }
 
 __global__ void hub_nch_k(const uint32_t* __restrict__ deg, uint32_t n_hub,
@@ -163,6 +184,8 @@ struct PrArgs {
   unsigned* hub_cnt;         // per hub: chunk arrivals this iteration
   double2* hub_contrib[2];   // per hub: (|next-rank|, dangling next)
   double2* block_part[2];    // per block
+  double2* totals;           // [2]: (delta, dangling) published by the barrier
+  uint32_t iso_lo;           // first isolated row
   unsigned* bar_count;
   unsigned* bar_gen;
   int* err;
@@ -181,6 +204,8 @@ struct Fin {
 struct PrSmem {
   float hot[kHot];
   double2 dsh[kPrWarps];
+  unsigned gen;
+  int last;
 };
 
 __device__ __forceinline__ double row_divisor(const PrArgs& a, uint64_t u) {
@@ -367,30 +392,56 @@ __device__ __forceinline__ Fin block_sum_fin(Fin v, double2* sh) {
 
 // Every block computes the same totals from the same partials in the same
 // order (warp 0, lane-strided, then a fixed shuffle tree).
-__device__ __forceinline__ Fin global_totals(const PrArgs& a, int p, double2* sh) {
-  if (threadIdx.x < 32) {
-    double d = 0.0, g = 0.0;
-    for (uint32_t i = threadIdx.x; i < gridDim.x; i += 32) {
-      double2 v = __ldcg(&a.block_part[p][i]);
-      d += v.x;
-      g += v.y;
-    }
-    for (uint32_t i = threadIdx.x; i < a.n_hub; i += 32) {
-      double2 v = __ldcg(&a.hub_contrib[p][i]);
-      d += v.x;
-      g += v.y;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      d += __shfl_down_sync(0xffffffffu, d, o);
-      g += __shfl_down_sync(0xffffffffu, g, o);
-    }
-    if (threadIdx.x == 0) sh[0] = make_double2(d, g);
+// Bounded grid barrier whose last-arriving block sums the partials of
+// parity p -- block partials, hub contributions, then `extra` (the isolated
+// rows' closed-form terms) -- thread-strided and through a fixed tree, so the
+// order does not depend on which block arrives last, and publishes the
+// totals; every block returns them.  A wait longer than kBarrierLimitNs sets
+// the error flag and returns.
+__device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm, Fin extra) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sm.gen = *(volatile unsigned*)a.bar_gen;
+    __threadfence();
+    sm.last = atomicAdd(a.bar_count, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  Fin r{sh[0].x, sh[0].y};
+  if (sm.last) {
+    __threadfence();
+    double d = 0.0, g = 0.0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += kPrBlock) {
+      const double2 v = __ldcg(&a.block_part[p][i]);
+      d += v.x;
+      g += v.y;
+    }
+    for (uint32_t i = threadIdx.x; i < a.n_hub; i += kPrBlock) {
+      const double2 v = __ldcg(&a.hub_contrib[p][i]);
+      d += v.x;
+      g += v.y;
+    }
+    const Fin r = block_sum_fin(Fin{d, g}, sm.dsh);
+    if (threadIdx.x == 0) {
+      a.totals[p] = make_double2(r.delta + extra.delta, r.dang + extra.dang);
+      __threadfence();
+      atomicExch(a.bar_count, 0u);
+      __threadfence();
+      atomicAdd(a.bar_gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    const uint64_t t0 = global_ns();
+    while (*(volatile unsigned*)a.bar_gen == sm.gen) {
+      __nanosleep(32);
+      if (global_ns() - t0 > kBarrierLimitNs) {
+        atomicExch(a.err, 1);
+        break;
+      }
+      if (*(volatile int*)a.err) break;
+    }
+    __threadfence();
+  }
   __syncthreads();
-  return r;
+  const double2 t = __ldcg(&a.totals[p]);
+  return Fin{t.x, t.y};
 }
 
 __device__ __forceinline__ void load_hot(const PrArgs& a, PrSmem& sm, int cur) {
@@ -438,9 +489,13 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     Fin b = block_sum_fin(f, sm.dsh);
     if (threadIdx.x == 0) a.block_part[0][blockIdx.x] = make_double2(0.0, b.dang);
   }
-  grid_barrier(a.bar_count, a.bar_gen, gridDim.x, a.err, kBarrierLimitNs);
-  Fin tot = global_totals(a, 0, sm.dsh);
+  // isolated rows (no in-edges, no out-edges): rank_0 = 1/n, dangling; on
+  // every iteration their rank is exactly `base` (base + d * 0)
+  const double n_iso = (double)(a.n - a.iso_lo);
+  const double r0 = 1.0 / nf;
+  Fin tot = barrier_totals(a, 0, sm, Fin{0.0, n_iso * r0});
   double dm = tot.dang;
+  double prev_iso = r0;
   int cur = 0;
   uint32_t iters = 0;
   double delta = 0.0;
@@ -455,14 +510,18 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     for (uint32_t u = gwarp; u < a.n_units; u += nwarps) run_unit<kW>(a, sm, u, cur, parity, base, f);
     Fin b = block_sum_fin(f, sm.dsh);
     if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = make_double2(b.delta, b.dang);
-    grid_barrier(a.bar_count, a.bar_gen, gridDim.x, a.err, kBarrierLimitNs);
-    tot = global_totals(a, parity, sm.dsh);
+    tot = barrier_totals(a, parity, sm, Fin{n_iso * fabs(base - prev_iso), n_iso * base});
+    prev_iso = base;
     delta = tot.delta;
     dm = tot.dang;
     cur ^= 1;
     iters++;
     if (delta < a.tol) break;  // every block sees the same delta
   }
+  // the isolated rows' final rank: the last iteration's base (1/n if none ran)
+  for (uint64_t u = a.iso_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.n;
+       u += (uint64_t)gridDim.x * kPrBlock)
+    a.rank[cur][u] = prev_iso;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *a.out_iters = iters;
     *a.out_delta = delta;
@@ -511,7 +570,7 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   // ---- relabel by in-degree, highest first (stable: ties keep id order)
   {
     Scratch<uint32_t> key(n, s), key_sorted(n, s);
-    neg_indeg_k<<<grid_for(n), kBlock, 0, s>>>(t->in.off.get(), n, key.get());
+    exec_order_key_k<<<grid_for(n), kBlock, 0, s>>>(t->in.off.get(), t->out.off.get(), n, key.get());
     UG_LAUNCH_CHECK();
     plan->old_of_new.alloc(n, s);
     radix_sort_pairs(key.get(), nullptr, n, 32, key_sorted.get(), plan->old_of_new.get(), nullptr,
@@ -537,10 +596,10 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
     UG_LAUNCH_CHECK();
   }
   // ---- degree classes (rows are sorted by degree, so each is a range)
-  uint32_t bounds[kClasses - 1];
+  uint32_t bounds[kClasses];
   {
-    Scratch<uint32_t> db(kClasses - 1, s);
-    class_bounds_k<<<1, 1, 0, s>>>(deg.get(), n, db.get());
+    Scratch<uint32_t> db(kClasses, s);
+    class_bounds_k<<<1, 1, 0, s>>>(deg.get(), plan->outdeg.get(), n, db.get());
     UG_LAUNCH_CHECK();
     UG_CUDA(cudaMemcpyAsync(bounds, db.get(), sizeof(bounds), cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));
@@ -550,8 +609,9 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   c.hi[0] = bounds[0];
   for (int k = 1; k < kClasses; k++) {
     c.lo[k] = bounds[k - 1];
-    c.hi[k] = k < kClasses - 1 ? bounds[k] : (uint32_t)n;
+    c.hi[k] = bounds[k];  // the last class stops at the isolated rows
   }
+  plan->iso_lo = bounds[kClasses - 1];
   plan->n_hub = c.hi[0];
   // hub chunks
   plan->hub_nch.alloc(plan->n_hub ? plan->n_hub : 1, s);
@@ -629,6 +689,7 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   Scratch<unsigned> hub_cnt(nh, s);
   Scratch<double2> hub_contrib(2 * (size_t)nh, s);
   Scratch<double2> block_part(2 * (size_t)G, s);
+  Scratch<double2> totals(2, s);
   Scratch<unsigned> ctl(8, s);  // bar_count, bar_gen, err, iters, buf
   Scratch<double> ctl_d(1, s);
   UG_CUDA(cudaMemsetAsync(hub_cnt.get(), 0, nh * sizeof(unsigned), s));
@@ -674,6 +735,8 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   a.hub_contrib[1] = hub_contrib.get() + nh;
   a.block_part[0] = block_part.get();
   a.block_part[1] = block_part.get() + G;
+  a.totals = totals.get();
+  a.iso_lo = plan->iso_lo;
   a.bar_count = ctl.get() + 0;
   a.bar_gen = ctl.get() + 1;
   a.err = (int*)(ctl.get() + 2);
