@@ -57,6 +57,7 @@ struct PrClassTable {
 struct PrPlan {
   PrClassTable cls{};
   uint32_t iso_lo = 0;  // rows [iso_lo, n) are isolated: rank follows in closed form
+  uint32_t zi_lo = 0;   // rows [zi_lo, n) have no in-edges: rank = base every iteration
   uint32_t n_units = 0, n_hub = 0, n_chunks = 0;
   DevArray<uint2> hub_unit;            // per hub chunk: {hub index, chunk}
   DevArray<uint32_t> hub_first, hub_nch;
@@ -125,7 +126,8 @@ __global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n,
 
 // Class boundaries over the non-increasing degree sequence: bounds[t] =
 // number of rows with degree > thr[t]; bounds[kClasses - 1] = first isolated
-// row (in- and out-degree 0; they end the execution order).
+// row (in- and out-degree 0; they end the execution order); bounds[kClasses]
+// = first row without in-edges.
 __global__ void class_bounds_k(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ outdeg,
                                uint64_t n, uint32_t* __restrict__ bounds) {
   const uint32_t thr[kClasses - 1] = {kHubDeg, 64u, 32u, 16u, 8u, 4u};
@@ -149,6 +151,16 @@ __global__ void class_bounds_k(const uint32_t* __restrict__ deg, const uint32_t*
       hi = mid;
   }
   bounds[kClasses - 1] = (uint32_t)lo;
+  lo = 0;
+  hi = n;  // first row without in-edges
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (deg[mid] != 0)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  bounds[kClasses] = (uint32_t)lo;
 }
 
 __global__ void hub_nch_k(const uint32_t* __restrict__ deg, uint32_t n_hub,
@@ -186,6 +198,7 @@ struct PrArgs {
   double2* block_part[2];    // per block
   double2* totals;           // [2]: (delta, dangling) published by the barrier
   uint32_t iso_lo;           // first isolated row
+  uint32_t zi_lo;            // first row without in-edges (<= iso_lo)
   unsigned* bar_count;
   unsigned* bar_gen;
   int* err;
@@ -455,6 +468,21 @@ __device__ __forceinline__ void load_hot(const PrArgs& a, PrSmem& sm, int cur) {
   __syncthreads();
 }
 
+// Sources without in-edges (rows [zi_lo, iso_lo)): their rank is `rank`
+// (closed form, not stored per iteration); only the share they pass on is
+// written, and a dangling one (weighted, all out-weights 0) adds its rank to
+// the dangling mass.  A coalesced pass over all threads of the grid.
+__device__ __forceinline__ void sources_without_in_edges(const PrArgs& a, double rank, int buf,
+                                                         Fin& f) {
+  for (uint64_t u = a.zi_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.iso_lo;
+       u += (uint64_t)gridDim.x * kPrBlock) {
+    const double div = row_divisor(a, u);
+    const bool dangling = !(div > 0.0);
+    a.x[buf][u] = dangling ? 0.f : (float)(rank / div);
+    if (dangling) f.dang += rank;
+  }
+}
+
 template <bool kW>
 __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -486,11 +514,14 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
         if (r < a.cls.hi[c] && lane % G == 0) init_row(a, r, r0, f);
       }
     }
+    sources_without_in_edges(a, r0, 0, f);
     Fin b = block_sum_fin(f, sm.dsh);
     if (threadIdx.x == 0) a.block_part[0][blockIdx.x] = make_double2(0.0, b.dang);
   }
-  // isolated rows (no in-edges, no out-edges): rank_0 = 1/n, dangling; on
-  // every iteration their rank is exactly `base` (base + d * 0)
+  // rows without in-edges: next = base + d * 0 = base on every iteration
+  // (1/n before the first), so their ranks follow in closed form; isolated
+  // rows (no out-edges either) are dangling and are never gathered
+  const double n_zi = (double)(a.n - a.zi_lo);
   const double n_iso = (double)(a.n - a.iso_lo);
   const double r0 = 1.0 / nf;
   Fin tot = barrier_totals(a, 0, sm, Fin{0.0, n_iso * r0});
@@ -508,9 +539,10 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     load_hot(a, sm, cur);
     Fin f{0.0, 0.0};
     for (uint32_t u = gwarp; u < a.n_units; u += nwarps) run_unit<kW>(a, sm, u, cur, parity, base, f);
+    sources_without_in_edges(a, base, cur ^ 1, f);
     Fin b = block_sum_fin(f, sm.dsh);
     if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = make_double2(b.delta, b.dang);
-    tot = barrier_totals(a, parity, sm, Fin{n_iso * fabs(base - prev_iso), n_iso * base});
+    tot = barrier_totals(a, parity, sm, Fin{n_zi * fabs(base - prev_iso), n_iso * base});
     prev_iso = base;
     delta = tot.delta;
     dm = tot.dang;
@@ -518,8 +550,8 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     iters++;
     if (delta < a.tol) break;  // every block sees the same delta
   }
-  // the isolated rows' final rank: the last iteration's base (1/n if none ran)
-  for (uint64_t u = a.iso_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.n;
+  // rows without in-edges: the last iteration's base (1/n if none ran)
+  for (uint64_t u = a.zi_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.n;
        u += (uint64_t)gridDim.x * kPrBlock)
     a.rank[cur][u] = prev_iso;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -596,9 +628,9 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
     UG_LAUNCH_CHECK();
   }
   // ---- degree classes (rows are sorted by degree, so each is a range)
-  uint32_t bounds[kClasses];
+  uint32_t bounds[kClasses + 1];
   {
-    Scratch<uint32_t> db(kClasses, s);
+    Scratch<uint32_t> db(kClasses + 1, s);
     class_bounds_k<<<1, 1, 0, s>>>(deg.get(), plan->outdeg.get(), n, db.get());
     UG_LAUNCH_CHECK();
     UG_CUDA(cudaMemcpyAsync(bounds, db.get(), sizeof(bounds), cudaMemcpyDeviceToHost, s));
@@ -609,9 +641,10 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   c.hi[0] = bounds[0];
   for (int k = 1; k < kClasses; k++) {
     c.lo[k] = bounds[k - 1];
-    c.hi[k] = bounds[k];  // the last class stops at the isolated rows
+    c.hi[k] = k < kClasses - 1 ? bounds[k] : bounds[kClasses];  // up to the rows without in-edges
   }
   plan->iso_lo = bounds[kClasses - 1];
+  plan->zi_lo = bounds[kClasses];
   plan->n_hub = c.hi[0];
   // hub chunks
   plan->hub_nch.alloc(plan->n_hub ? plan->n_hub : 1, s);
@@ -737,6 +770,7 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   a.block_part[1] = block_part.get() + G;
   a.totals = totals.get();
   a.iso_lo = plan->iso_lo;
+  a.zi_lo = plan->zi_lo;
   a.bar_count = ctl.get() + 0;
   a.bar_gen = ctl.get() + 1;
   a.err = (int*)(ctl.get() + 2);
