@@ -36,6 +36,7 @@
 #include "frontier.cuh"
 #include "primitives.cuh"
 #include "batch.cuh"
+#include "fixedpoint.cuh"
 #include "unionfind.cuh"
 
 namespace ug {
@@ -47,8 +48,6 @@ constexpr int kBkMaxBuckets = 3;
 // parents or counts), leaving room for the static reduction area.
 constexpr uint32_t kBkSmemBytesMax = 224u * 1024u;
 
-typedef unsigned __int128 u128;
-
 struct BkShared {
   GraphDesc g;
   unsigned long long red[4 * 32];
@@ -57,32 +56,6 @@ struct BkShared {
   uint32_t range[2];
   uint32_t item;
 };
-
-// v >= 0 finite -> floor(v * 2^96) (0 for subnormals), saturating.
-__device__ __forceinline__ u128 fx_of(double v) {
-  const uint64_t b = (uint64_t)__double_as_longlong(v);
-  const int e = (int)((b >> 52) & 0x7ff);
-  if (e == 0) return 0;
-  const uint64_t mant = (b & 0xFFFFFFFFFFFFFull) | (1ull << 52);
-  const int sh = e - 1075 + 96;  // v * 2^96 = mant * 2^sh
-  if (sh >= 75) return ~(u128)0;
-  if (sh >= 0) return (u128)mant << sh;
-  if (sh <= -53) return 0;
-  return (u128)(mant >> -sh);
-}
-
-__device__ __forceinline__ double fx_value(u128 x) {
-  const double hi = __ull2double_rn((unsigned long long)(x >> 64));
-  const double lo = __ull2double_rn((unsigned long long)x);
-  return __dmul_rn(__dadd_rn(__dmul_rn(hi, 0x1p64), lo), 0x1p-96);
-}
-
-__device__ __forceinline__ u128 shfl_down_u128(u128 v, int o) {
-  unsigned long long lo = (unsigned long long)v, hi = (unsigned long long)(v >> 64);
-  lo = __shfl_down_sync(0xffffffffu, lo, o);
-  hi = __shfl_down_sync(0xffffffffu, hi, o);
-  return ((u128)hi << 64) | lo;
-}
 
 // Block sum of two fixed-point accumulators; every thread gets the f64
 // values.  Integer addition is exact, so the order does not matter.

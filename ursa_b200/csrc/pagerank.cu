@@ -32,6 +32,7 @@
 //    order, so runs are bit-reproducible.
 #include <cmath>
 
+#include "fixedpoint.cuh"
 #include "primitives.cuh"
 #include "topo.cuh"
 
@@ -46,6 +47,7 @@ constexpr int kHot = 32768;           // shares cached in shared memory (128 KB)
 constexpr int kClasses = 7;           // hub, G = 32, 16, 8, 4, 2, 1
 constexpr int kBatchWide = 8;         // loads in flight per lane, 32-lane rows
 constexpr int kBatchHub = 16;         // loads in flight per lane, hub chunks
+constexpr int kUnitsPerGrab = 8;      // units a warp takes from its block's counter
 constexpr uint64_t kBarrierLimitNs = 5000000000ull;  // 5 s per grid barrier wait
 }  // namespace
 
@@ -194,8 +196,8 @@ struct PrArgs {
   uint32_t n_hub;
   F2* chunk_part;            // per hub chunk
   unsigned* hub_cnt;         // per hub: chunk arrivals this iteration
-  double2* hub_contrib[2];   // per hub: (|next-rank|, dangling next)
-  double2* block_part[2];    // per block
+  ulonglong2* hub_contrib[2];  // per hub: (|next-rank|, dangling next), fixed point
+  ulonglong2* block_part[2];   // per block, fixed point
   double2* totals;           // [2]: (delta, dangling) published by the barrier
   uint32_t iso_lo;           // first isolated row
   uint32_t zi_lo;            // first row without in-edges (<= iso_lo)
@@ -214,11 +216,19 @@ struct Fin {
   double delta, dang;
 };
 
+// Per-thread fixed-point accumulators of |next - rank| and of the dangling
+// rows' next ranks (64-bit, scale 2^-58: order-independent; every partial
+// sum is below its total, and the totals are at most 2 and 1).
+struct Fx {
+  unsigned long long delta, dang;
+};
+
 struct PrSmem {
   float hot[kHot];
-  double2 dsh[kPrWarps];
+  ulonglong2 red[kPrWarps];
   unsigned gen;
   int last;
+  unsigned next;  // work counter of the block (dynamic unit scheduling)
 };
 
 __device__ __forceinline__ double row_divisor(const PrArgs& a, uint64_t u) {
@@ -226,22 +236,22 @@ __device__ __forceinline__ double row_divisor(const PrArgs& a, uint64_t u) {
 }
 
 __device__ __forceinline__ void finish_row(const PrArgs& a, uint64_t u, double sum, double old,
-                                           double div, double base, int cur, Fin& f) {
+                                           double div, double base, int cur, Fx& f) {
   // next[u] = base + d * contrib(u)   (pagerank.rs:81-83)
   double nx = __dadd_rn(base, __dmul_rn(a.damping, sum));
-  f.delta += fabs(nx - old);
+  f.delta += fx64_of(fabs(__dsub_rn(nx, old)));
   a.rank[cur ^ 1][u] = nx;
   bool dangling = !(div > 0.0);
   a.x[cur ^ 1][u] = dangling ? 0.f : (float)(nx / div);
-  if (dangling) f.dang += nx;
+  if (dangling) f.dang += fx64_of(nx);
 }
 
-__device__ __forceinline__ void init_row(const PrArgs& a, uint64_t u, double r0, Fin& f) {
+__device__ __forceinline__ void init_row(const PrArgs& a, uint64_t u, double r0, Fx& f) {
   a.rank[0][u] = r0;
   double div = row_divisor(a, u);
   bool dangling = !(div > 0.0);
   a.x[0][u] = dangling ? 0.f : (float)(r0 / div);
-  if (dangling) f.dang += r0;
+  if (dangling) f.dang += fx64_of(r0);
 }
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
@@ -302,7 +312,7 @@ __device__ __forceinline__ F2 group_sum(F2 v) {
 template <int G, bool kW>
 __device__ __forceinline__ void class_unit(const PrArgs& a, const PrSmem& sm, uint32_t lo,
                                            uint32_t hi, uint32_t unit, int cur, double base,
-                                           Fin& f) {
+                                           Fx& f) {
   const int lane = threadIdx.x & 31;
   const int sub = lane % G;
   const uint32_t r = lo + unit * (32u / G) + (uint32_t)(lane / G);
@@ -356,16 +366,16 @@ __device__ __forceinline__ void hub_unit(const PrArgs& a, const PrSmem& sm, uint
       }
     }
     if (finish) {
-      Fin g{0.0, 0.0};
+      Fx g{0, 0};
       finish_row(a, r, f2_value(row), a.rank[cur][r], row_divisor(a, r), base, cur, g);
-      a.hub_contrib[parity][hu.x] = make_double2(g.delta, g.dang);
+      a.hub_contrib[parity][hu.x] = make_ulonglong2(g.delta, g.dang);
     }
   }
 }
 
 template <bool kW>
 __device__ __forceinline__ void run_unit(const PrArgs& a, const PrSmem& sm, uint32_t u, int cur,
-                                         int parity, double base, Fin& f) {
+                                         int parity, double base, Fx& f) {
   int c = 0;
 #pragma unroll
   for (int k = 1; k < kClasses; k++)
@@ -383,8 +393,8 @@ __device__ __forceinline__ void run_unit(const PrArgs& a, const PrSmem& sm, uint
   }
 }
 
-// Fixed-order block reduction of two doubles; result valid in thread 0.
-__device__ __forceinline__ Fin block_sum_fin(Fin v, double2* sh) {
+// Block sum of the fixed-point accumulators; result valid in thread 0.
+__device__ __forceinline__ Fx block_sum_fx(Fx v, ulonglong2* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -392,9 +402,9 @@ __device__ __forceinline__ Fin block_sum_fin(Fin v, double2* sh) {
     v.dang += __shfl_down_sync(0xffffffffu, v.dang, o);
   }
   __syncthreads();
-  if (lane == 0) sh[w] = make_double2(v.delta, v.dang);
+  if (lane == 0) sh[w] = make_ulonglong2(v.delta, v.dang);
   __syncthreads();
-  Fin r{0.0, 0.0};
+  Fx r{0, 0};
   if (threadIdx.x == 0)
     for (int i = 0; i < kPrWarps; i++) {
       r.delta += sh[i].x;
@@ -403,14 +413,12 @@ __device__ __forceinline__ Fin block_sum_fin(Fin v, double2* sh) {
   return r;
 }
 
-// Every block computes the same totals from the same partials in the same
-// order (warp 0, lane-strided, then a fixed shuffle tree).
-// Bounded grid barrier whose last-arriving block sums the partials of
-// parity p -- block partials, hub contributions, then `extra` (the isolated
-// rows' closed-form terms) -- thread-strided and through a fixed tree, so the
-// order does not depend on which block arrives last, and publishes the
-// totals; every block returns them.  A wait longer than kBarrierLimitNs sets
-// the error flag and returns.
+// Bounded grid barrier whose last-arriving block sums the fixed-point
+// partials of parity p (block partials and hub contributions; exact, so the
+// result does not depend on which block arrives last or which warp did which
+// unit), adds `extra` (the closed-form terms of the rows without in-edges)
+// and publishes the totals; every block returns them.  A wait longer than
+// kBarrierLimitNs sets the error flag and returns.
 __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm, Fin extra) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -421,20 +429,21 @@ __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm
   __syncthreads();
   if (sm.last) {
     __threadfence();
-    double d = 0.0, g = 0.0;
+    Fx acc{0, 0};
     for (uint32_t i = threadIdx.x; i < gridDim.x; i += kPrBlock) {
-      const double2 v = __ldcg(&a.block_part[p][i]);
-      d += v.x;
-      g += v.y;
+      const ulonglong2 v = __ldcg(&a.block_part[p][i]);
+      acc.delta += v.x;
+      acc.dang += v.y;
     }
     for (uint32_t i = threadIdx.x; i < a.n_hub; i += kPrBlock) {
-      const double2 v = __ldcg(&a.hub_contrib[p][i]);
-      d += v.x;
-      g += v.y;
+      const ulonglong2 v = __ldcg(&a.hub_contrib[p][i]);
+      acc.delta += v.x;
+      acc.dang += v.y;
     }
-    const Fin r = block_sum_fin(Fin{d, g}, sm.dsh);
+    const Fx r = block_sum_fx(acc, sm.red);
     if (threadIdx.x == 0) {
-      a.totals[p] = make_double2(r.delta + extra.delta, r.dang + extra.dang);
+      a.totals[p] = make_double2(__dadd_rn(fx64_value(r.delta), extra.delta),
+                                 __dadd_rn(fx64_value(r.dang), extra.dang));
       __threadfence();
       atomicExch(a.bar_count, 0u);
       __threadfence();
@@ -473,13 +482,13 @@ __device__ __forceinline__ void load_hot(const PrArgs& a, PrSmem& sm, int cur) {
 // written, and a dangling one (weighted, all out-weights 0) adds its rank to
 // the dangling mass.  A coalesced pass over all threads of the grid.
 __device__ __forceinline__ void sources_without_in_edges(const PrArgs& a, double rank, int buf,
-                                                         Fin& f) {
+                                                         Fx& f) {
   for (uint64_t u = a.zi_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.iso_lo;
        u += (uint64_t)gridDim.x * kPrBlock) {
     const double div = row_divisor(a, u);
     const bool dangling = !(div > 0.0);
     a.x[buf][u] = dangling ? 0.f : (float)(rank / div);
-    if (dangling) f.dang += rank;
+    if (dangling) f.dang += fx64_of(rank);
   }
 }
 
@@ -493,7 +502,7 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
   const int lane = threadIdx.x & 31;
   // ---- prologue: rank_0 = 1/n, shares, dangling mass of rank_0
   {
-    Fin f{0.0, 0.0};
+    Fx f{0, 0};
     const double r0 = 1.0 / nf;
     for (uint32_t u = gwarp; u < a.n_units; u += nwarps) {
       int c = 0;
@@ -504,9 +513,9 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
       if (c == 0) {
         const uint2 hu = a.hub_unit[unit];
         if (hu.y == 0 && lane == 0) {
-          Fin g{0.0, 0.0};
+          Fx g{0, 0};
           init_row(a, a.cls.lo[0] + hu.x, r0, g);
-          a.hub_contrib[0][hu.x] = make_double2(0.0, g.dang);
+          a.hub_contrib[0][hu.x] = make_ulonglong2(0ull, g.dang);
         }
       } else {
         const int G = 32 >> (c - 1);
@@ -515,8 +524,8 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
       }
     }
     sources_without_in_edges(a, r0, 0, f);
-    Fin b = block_sum_fin(f, sm.dsh);
-    if (threadIdx.x == 0) a.block_part[0][blockIdx.x] = make_double2(0.0, b.dang);
+    const Fx b = block_sum_fx(f, sm.red);
+    if (threadIdx.x == 0) a.block_part[0][blockIdx.x] = make_ulonglong2(0ull, b.dang);
   }
   // rows without in-edges: next = base + d * 0 = base on every iteration
   // (1/n before the first), so their ranks follow in closed form; isolated
@@ -536,12 +545,27 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     // base = (1-d)/n + d*dangling_mass/n   (pagerank.rs:79)
     const double base = __dadd_rn(__ddiv_rn(1.0 - a.damping, nf),
                                   __ddiv_rn(__dmul_rn(a.damping, dm), nf));
-    load_hot(a, sm, cur);
-    Fin f{0.0, 0.0};
-    for (uint32_t u = gwarp; u < a.n_units; u += nwarps) run_unit<kW>(a, sm, u, cur, parity, base, f);
+    if (threadIdx.x == 0) sm.next = 0;
+    load_hot(a, sm, cur);  // ends with a block barrier
+    Fx f{0, 0};
+    // blocks own interleaved units (u = block + k * grid); warps of a block
+    // take kUnitsPerGrab of them at a time from the block's counter
+    for (bool done = false; !done;) {
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&sm.next, (unsigned)kUnitsPerGrab);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      for (uint32_t q = 0; q < (uint32_t)kUnitsPerGrab; q++) {
+        const uint32_t u = blockIdx.x + (k + q) * gridDim.x;
+        if (u >= a.n_units) {
+          done = true;
+          break;
+        }
+        run_unit<kW>(a, sm, u, cur, parity, base, f);
+      }
+    }
     sources_without_in_edges(a, base, cur ^ 1, f);
-    Fin b = block_sum_fin(f, sm.dsh);
-    if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = make_double2(b.delta, b.dang);
+    const Fx b = block_sum_fx(f, sm.red);
+    if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = make_ulonglong2(b.delta, b.dang);
     tot = barrier_totals(a, parity, sm, Fin{n_zi * fabs(base - prev_iso), n_iso * base});
     prev_iso = base;
     delta = tot.delta;
@@ -720,13 +744,13 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   Scratch<float> x(2 * n_pad, s);
   Scratch<F2> chunk_part(plan->n_chunks ? plan->n_chunks : 1, s);
   Scratch<unsigned> hub_cnt(nh, s);
-  Scratch<double2> hub_contrib(2 * (size_t)nh, s);
-  Scratch<double2> block_part(2 * (size_t)G, s);
+  Scratch<ulonglong2> hub_contrib(2 * (size_t)nh, s);
+  Scratch<ulonglong2> block_part(2 * (size_t)G, s);
   Scratch<double2> totals(2, s);
   Scratch<unsigned> ctl(8, s);  // bar_count, bar_gen, err, iters, buf
   Scratch<double> ctl_d(1, s);
   UG_CUDA(cudaMemsetAsync(hub_cnt.get(), 0, nh * sizeof(unsigned), s));
-  UG_CUDA(cudaMemsetAsync(hub_contrib.get(), 0, 2 * (size_t)nh * sizeof(double2), s));
+  UG_CUDA(cudaMemsetAsync(hub_contrib.get(), 0, 2 * (size_t)nh * sizeof(ulonglong2), s));
   UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 8 * sizeof(unsigned), s));
 
   Scratch<double> out_str;
