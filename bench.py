@@ -70,7 +70,7 @@ WORKLOAD = "rmat22_pagerank"
 # dram__bytes_read.sum + dram__bytes_write.sum of one pr_persistent_k launch on
 # this workload (prologue + 5 fixed iterations), from the ncu capture
 # summarised in profiles/pagerank_rmat22.md.
-NCU_TRAFFIC = {"bytes_per_launch": 1_685_397_000 + 261_330_176, "iterations": 5}
+NCU_TRAFFIC = {"bytes_per_launch": 1_341_229_000 + 55_156_736, "iterations": 5}
 
 
 def env_int(name, default):
@@ -400,9 +400,12 @@ def run_serve(args, rank, world):
             elif kind[i] == 1:
                 tickets.append(srv.hop(int(a[i]), 2))
             else:
+                # pick and submit under the lock: the uploader removes an id
+                # from `live` (under it) before releasing the graph, and the
+                # submitted query keeps the graph until it finishes
                 with live_lock:
                     gid = live[int(b[i]) % len(live)]
-                tickets.append(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
+                    tickets.append(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
         offered = count / (time.perf_counter() - t0)
         for t in tickets:
             infos.append(srv.result(t, timeout_s=600))
@@ -421,34 +424,40 @@ def run_serve(args, rank, world):
                 out[name] = {"p50_ms": float(np.percentile(sel, 50)), "p99_ms": float(np.percentile(sel, 99))}
         return out
 
-    drive(2000, 2000, 1)  # warm-up
-    launches0 = L.ursa_gpu_launch_count()
-    uuid = None
     try:
-        uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
-    except Exception:
-        pass
-    sampler = ClockSampler(uuid) if rank == 0 else None
-    if sampler:
-        sampler.start()
-        time.sleep(0.3)
-    sweep = []
-    total_q = 0
-    for j, rate in enumerate(SERVE_RATES):
-        count = int(min(max(rate * 3, 3000), 60000))
-        infos, offered, kind = drive(rate, count, 100 + j)
-        total_q += count
-        row = {"rate_qps": rate, "offered_qps": offered, "queries": count}
-        row.update(summarize(infos, kind))
-        sweep.append(row)
-    # closed loop: everything submitted at once (maximum sustained throughput)
-    infos, offered, kind = drive(1e9, 60000, 999)
-    total_q += 60000
-    closed = summarize(infos, kind)
-    clocks = sampler.stop() if sampler else None
-    launches = L.ursa_gpu_launch_count() - launches0
-    stats = srv.stats()
+        drive(2000, 2000, 1)  # warm-up
+        launches0 = L.ursa_gpu_launch_count()
+        uuid = None
+        try:
+            uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+        except Exception:
+            pass
+        sampler = ClockSampler(uuid) if rank == 0 else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        sweep = []
+        total_q = 0
+        for j, rate in enumerate(SERVE_RATES):
+            count = int(min(max(rate * 3, 3000), 60000))
+            infos, offered, kind = drive(rate, count, 100 + j)
+            total_q += count
+            row = {"rate_qps": rate, "offered_qps": offered, "queries": count}
+            row.update(summarize(infos, kind))
+            sweep.append(row)
+        # closed loop: everything submitted at once (maximum sustained throughput)
+        infos, offered, kind = drive(1e9, 60000, 999)
+        total_q += 60000
+        closed = summarize(infos, kind)
+        clocks = sampler.stop() if sampler else None
+        launches = L.ursa_gpu_launch_count() - launches0
+        stats = srv.stats()
 
+    except BaseException:
+        stop_up.set()
+        upt.join(timeout=30)
+        srv.close()
+        raise
     # the server (and its uploads) go before the plain path is timed
     stop_up.set()
     upt.join(timeout=30)
@@ -531,7 +540,7 @@ def run_batch(args, rank, world):
 
     L = _lib.load()
     _lib.check(L.ursa_gpu_set_device(local_rank))
-    n, k, s, d = batch_graphs()
+    n, k, s, d = batch_graphs(args.batch_count)
     G, N, M = len(n), int(n.sum()), int(k.sum())
     params = PageRankParams(DAMPING, MAX_ITER, TOL)
     h_s = torch.from_numpy(s).pin_memory()
@@ -545,7 +554,10 @@ def run_batch(args, rank, world):
         return h
 
     b = GraphBatch(n, k, s, d)
-    cfg, tuned_ms = b.tune(params)
+    if args.no_tune:
+        cfg, tuned_ms = b.config(), None
+    else:
+        cfg, tuned_ms = b.tune(params)
     stream = torch.cuda.Stream()
     for _ in range(max(args.warmup, 3)):
         b.run(params, stream=stream.cuda_stream)
@@ -614,22 +626,24 @@ def run_batch(args, rank, world):
             e2e.append(time.perf_counter() - t0)
 
     # the per-graph plain loop over the same graphs
-    off = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
-    t0 = time.perf_counter()
-    tops = [Topology.build(int(n[i]), s[off[i]:off[i + 1]], d[off[i]:off[i + 1]]) for i in range(G)]
-    plain_build_s = time.perf_counter() - t0
+    plain_s = plain_build_s = float("nan")
+    if not args.no_plain:
+        off = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
+        t0 = time.perf_counter()
+        tops = [Topology.build(int(n[i]), s[off[i]:off[i + 1]], d[off[i]:off[i + 1]]) for i in range(G)]
+        plain_build_s = time.perf_counter() - t0
 
-    def plain_pass():
-        for t in tops:
-            algo.pagerank(t, params)
-            algo.connected_components_weak(t)
-            algo.triangle_count(t)
+        def plain_pass():
+            for t in tops:
+                algo.pagerank(t, params)
+                algo.connected_components_weak(t)
+                algo.triangle_count(t)
 
-    plain_pass()  # plans, lazily built CSRs, pool
-    t0 = time.perf_counter()
-    plain_pass()
-    plain_s = time.perf_counter() - t0
-    del tops
+        plain_pass()  # plans, lazily built CSRs, pool
+        t0 = time.perf_counter()
+        plain_pass()
+        plain_s = time.perf_counter() - t0
+        del tops
 
     if rank == 0:
         ms = statistics.median(step_ms)
@@ -649,7 +663,8 @@ def run_batch(args, rank, world):
             "vs_baseline": None,
             "dtype": "f32-compensated SpMV, f64 ranks/residual; u32 components and triangle counts",
             "data": "synthetic",
-            "config": {"workload": BATCH_WORKLOAD, "graphs": G, "n_nodes": N, "n_edges": M,
+            "config": {"workload": BATCH_WORKLOAD if G == BATCH_COUNT else f"rmat_batch{G}_pr_cc_tc",
+                       "graphs": G, "n_nodes": N, "n_edges": M,
                        "damping": DAMPING, "tol": TOL, "max_iter": MAX_ITER,
                        "pagerank_iterations": {"min": int(iters.min()), "median": float(np.median(iters)),
                                                "max": int(iters.max()), "sum": int(iters.sum())},
@@ -659,12 +674,14 @@ def run_batch(args, rank, world):
             "e2e": {"value": G / statistics.median(e2e), "unit": "graphs/s",
                     "h2d_bytes_per_step": 8 * M + 16 * G, "d2h_bytes_per_step": 16 * N + 12 * G,
                     "ms_per_step": 1e3 * statistics.median(e2e)},
-            "plain_loop": {"graphs_per_s": G / plain_s, "s": plain_s, "build_s": plain_build_s,
-                           "e2e_graphs_per_s": G / (plain_s + plain_build_s),
-                           "calls": "Topology per graph; pagerank + connected_components_weak + "
-                                    "triangle_count per graph, host outputs"},
-            "speedup_vs_plain": {"device": (G / (ms * 1e-3)) / (G / plain_s),
-                                 "e2e": (G / statistics.median(e2e)) / (G / (plain_s + plain_build_s))},
+            "plain_loop": None if args.no_plain else {
+                "graphs_per_s": G / plain_s, "s": plain_s, "build_s": plain_build_s,
+                "e2e_graphs_per_s": G / (plain_s + plain_build_s),
+                "calls": "Topology per graph; pagerank + connected_components_weak + triangle_count per graph, "
+                         "host outputs"},
+            "speedup_vs_plain": None if args.no_plain else {
+                "device": (G / (ms * 1e-3)) / (G / plain_s),
+                "e2e": (G / statistics.median(e2e)) / (G / (plain_s + plain_build_s))},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "batch_k (pagerank-only launch)", "achieved": pr_achieved,
                          "peak": peak, "unit": "GB/s", "frac": pr_achieved / peak, "peak_kind": peak_kind,
@@ -685,6 +702,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # profiling aids (defaults give the benchmark above)
+    ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="pagerank max_iter (rmat22 workload)")
+    ap.add_argument("--tol", type=float, default=TOL, help="pagerank tol (rmat22 workload; 0 = fixed count)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (rmat22 workload)")
+    ap.add_argument("--batch-count", type=int, default=BATCH_COUNT, help="graphs in the batch workload")
+    ap.add_argument("--no-tune", action="store_true", help="batch workload: keep the default launch shapes")
+    ap.add_argument("--no-plain", action="store_true", help="batch workload: skip the per-graph plain loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -723,7 +747,7 @@ def main():
     _lib.check(L.ursa_gpu_set_device(local_rank))
     n, src, dst = make_workload()
     m = int(src.size)
-    params = PageRankParams(DAMPING, MAX_ITER, TOL)
+    params = PageRankParams(DAMPING, args.max_iter, args.tol)
 
     # ---- value: topology resident, device output
     topo = Topology.build(n, src, dst)
@@ -786,15 +810,16 @@ def main():
             L.ursa_gpu_topo_free(h)
         return st.iterations
 
-    for _ in range(max(min(args.warmup, 2), 1)):
-        e2e_step()
-    torch.cuda.synchronize()
     e2e_times, e2e_iters = [], []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        it = e2e_step()
-        e2e_times.append(time.perf_counter() - t0)
-        e2e_iters.append(it)
+    if not args.no_e2e:
+        for _ in range(max(min(args.warmup, 2), 1)):
+            e2e_step()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            it = e2e_step()
+            e2e_times.append(time.perf_counter() - t0)
+            e2e_iters.append(it)
 
     # ---- max over ranks
     t_dev = total_ms
@@ -834,10 +859,10 @@ def main():
             "vs_baseline": None,
             "dtype": "f32-compensated SpMV, f64 ranks/residual",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": TOL,
-                       "max_iter": MAX_ITER, "iterations": iters, "l2": "inputs larger than L2 (in-CSR 261 MB)",
+            "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": args.tol,
+                       "max_iter": args.max_iter, "iterations": iters, "l2": "inputs larger than L2 (in-CSR 261 MB)",
                        "parallelism": "replicas" if world > 1 else "single"},
-            "e2e": {"value": e2e_edges_all / t_e2e / 1e9, "unit": "GTEPS",
+            "e2e": None if not e2e_times else {"value": e2e_edges_all / t_e2e / 1e9, "unit": "GTEPS",
                     "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * n,
                     "ms_per_step": 1e3 * t_e2e / args.steps},
             "gpu_launches": int(launches),

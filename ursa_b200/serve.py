@@ -9,7 +9,9 @@ seed (algo/hop.rs:52-130) and pagerank (algo/pagerank.rs:98-124).
 
 from __future__ import annotations
 
+import atexit
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -18,6 +20,20 @@ from . import _lib
 from ._lib import QUERY_HOP, QUERY_PAGERANK, QUERY_SHORTEST_PATH, PageRankParams, Query, QueryInfo, ServerConfig
 
 __all__ = ["Server", "Completed", "QUERY_SHORTEST_PATH", "QUERY_HOP", "QUERY_PAGERANK"]
+
+# Servers still open at interpreter exit are closed before the CUDA runtime
+# shuts down (a server's scheduler thread and resident kernels must not
+# outlive it).
+_open_servers: "weakref.WeakSet[Server]" = weakref.WeakSet()
+
+
+@atexit.register
+def _close_open_servers() -> None:
+    for srv in list(_open_servers):
+        try:
+            srv.close()
+        except Exception:
+            pass
 
 
 @dataclass
@@ -48,7 +64,7 @@ class Server:
         _lib.check(_lib.load().ursa_gpu_server_create(resident.handle if resident is not None else None,
                                                       C.byref(cfg), C.byref(h)))
         self._h = h
-        self._buf_u32 = np.empty(1 << 16, np.uint32)
+        _open_servers.add(self)
 
     @property
     def handle(self):
