@@ -216,6 +216,42 @@ int ursa_gpu_betweenness_weighted(ursa_gpu_topo *t, const double *weights, uint6
                                   double *out);
 
 /* ------------------------------------------------------------------------
+ * Node-id interning on the device.
+ *
+ * IdMap::from_edge_batches / from_edge_arrays for Int64 ids
+ * (ursa-core/src/id_map.rs:197-320): the edges' user ids, chunk after chunk,
+ * become dense u32 ids in first-seen order (per edge, src before dst), as
+ * the ingress path does before Topology::build (ursa-plan/src/topology.rs:
+ * 39-45).  The caller rejects null endpoints first, as the reference does
+ * (IdError::Null).  String (Utf8) ids stay on the host.
+ * ---------------------------------------------------------------------- */
+typedef struct ursa_gpu_idmap ursa_gpu_idmap;
+
+/* Interns n_chunks chunks of (src, dst) Int64 value buffers (host), each
+ * chunk_lens[c] rows; at most 2^29 edges in all. */
+int ursa_gpu_idmap_build(uint64_t n_chunks, const int64_t *const *src_chunks,
+                         const int64_t *const *dst_chunks, const uint64_t *chunk_lens,
+                         ursa_gpu_idmap **out);
+void ursa_gpu_idmap_free(ursa_gpu_idmap *m);
+/* IdMap::len (id_map.rs:443) and the number of interned edges. */
+uint64_t ursa_gpu_idmap_len(const ursa_gpu_idmap *m);
+uint64_t ursa_gpu_idmap_n_edges(const ursa_gpu_idmap *m);
+/* IdMap::user_id_array (id_map.rs:359): the user ids in dense order. */
+int ursa_gpu_idmap_user_ids(ursa_gpu_idmap *m, int64_t *out);
+/* The edges in dense ids (the Vec<u32> pair from_edge_batches returns). */
+int ursa_gpu_idmap_dense_edges(ursa_gpu_idmap *m, uint32_t *src_out, uint32_t *dst_out);
+/* Topology::build(len, dense src, dense dst) straight from the device
+ * columns (no host round trip). */
+int ursa_gpu_idmap_topology(ursa_gpu_idmap *m, ursa_gpu_topo **out);
+/* IdMap::gather_user (id_map.rs:381): user ids of dense indices
+ * (URSA_GPU_EINVAL on an index >= len). */
+int ursa_gpu_idmap_gather_user(ursa_gpu_idmap *m, const uint32_t *dense, uint64_t n, int64_t *out);
+/* IdMap::dense_from_array (id_map.rs:402) for Int64 ids: found[i] = 0 where
+ * the id is not in the map (the reference's None). */
+int ursa_gpu_idmap_lookup(ursa_gpu_idmap *m, const int64_t *ids, uint64_t n, uint32_t *dense_out,
+                          uint8_t *found);
+
+/* ------------------------------------------------------------------------
  * Batched execution of many small independent graphs.
  *
  * The reference runs one graph per Topology: Topology::build

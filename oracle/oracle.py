@@ -73,6 +73,8 @@ def lib():
         L.orc_sample_indices.argtypes = [u64, u64, i32, u64, P]
         L.orc_sample_sources.restype = u64
         L.orc_sample_sources.argtypes = [u64, i32, f64, i32, u64, P]
+        L.orc_idmap_build.restype = u64
+        L.orc_idmap_build.argtypes = [P, P, u64, P, P, P]
         L.orc_set_threads.argtypes = [i32]
         L.orc_get_threads.restype = i32
         _lib = L
@@ -263,3 +265,18 @@ def sample_sources(n: int, sample=None, seed=None) -> np.ndarray:
     out = np.empty(max(n, 1), np.uint32)
     k = lib().orc_sample_sources(n, sample is not None, float(sample or 0.0), seed is not None, int(seed or 0), _p(out))
     return out[:k].copy()
+
+
+def idmap_build(src, dst):
+    """IdMap::from_edge_arrays / from_edge_batches for Int64 ids
+    (ursa-core/src/id_map.rs:197-320): (to_user i64[n], dense_src u32[m],
+    dense_dst u32[m]); chunked input is the same as its concatenation."""
+    s = np.ascontiguousarray(np.asarray(src, dtype=np.int64))
+    d = np.ascontiguousarray(np.asarray(dst, dtype=np.int64))
+    if s.shape != d.shape:
+        raise ValueError("src and dst columns must have the same length")
+    ds = np.empty(s.size, np.uint32)
+    dd = np.empty(s.size, np.uint32)
+    users = np.empty(2 * s.size, np.int64)
+    k = lib().orc_idmap_build(_p(s), _p(d), s.size, _p(ds), _p(dd), _p(users))
+    return users[:k].copy(), ds, dd

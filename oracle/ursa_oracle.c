@@ -1367,3 +1367,49 @@ void orc_betweenness_sources(orc_topo *t, const double *weights,
   if (t->n == 0) return;
   accumulate_sources(t, weights, sources, k, out);
 }
+
+/* ------------------------------------------------------------------------ */
+/* IdMap::from_edge_batches for Int64 ids (id_map.rs:220-260, intern_i64     */
+/* :294-320): edges are visited in chunk order and, per edge, src is interned */
+/* before dst; an id's dense index is the number of distinct ids seen before  */
+/* its first occurrence.  The reference uses an FxHashMap; the order of the   */
+/* result depends only on first occurrences, so any exact map gives the same  */
+/* output.  Here: open addressing over 2^k slots with linear probing.         */
+/* ------------------------------------------------------------------------ */
+static uint64_t idmap_mix(uint64_t x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return x;
+}
+
+uint64_t orc_idmap_build(const int64_t *src, const int64_t *dst, uint64_t n_edges,
+                         uint32_t *dense_src, uint32_t *dense_dst, int64_t *to_user) {
+  uint64_t cap = 16;
+  while (cap < 4 * n_edges + 16) cap <<= 1;
+  int64_t *keys = (int64_t *)malloc(cap * sizeof(int64_t));
+  uint32_t *vals = (uint32_t *)malloc(cap * sizeof(uint32_t));
+  unsigned char *used = (unsigned char *)calloc(cap, 1);
+  uint64_t next = 0;
+  for (uint64_t i = 0; i < 2 * n_edges; i++) {
+    const int64_t key = (i & 1) ? dst[i >> 1] : src[i >> 1];
+    uint64_t h = idmap_mix((uint64_t)key) & (cap - 1);
+    while (used[h] && keys[h] != key) h = (h + 1) & (cap - 1);
+    if (!used[h]) {
+      used[h] = 1;
+      keys[h] = key;
+      vals[h] = (uint32_t)next;
+      to_user[next++] = key;
+    }
+    if (i & 1)
+      dense_dst[i >> 1] = vals[h];
+    else
+      dense_src[i >> 1] = vals[h];
+  }
+  free(keys);
+  free(vals);
+  free(used);
+  return next;
+}

@@ -25,6 +25,11 @@ extern "C" {
 typedef struct orc_topo orc_topo;
 
 /* Worker threads used by the parallel sweeps (results do not depend on it). */
+/* IdMap::from_edge_batches, Int64 ids (id_map.rs:220-320): dense ids in
+ * first-seen order over src[0], dst[0], src[1], dst[1], ...; to_user holds up
+ * to 2 * n_edges ids; returns the number of distinct ids. */
+uint64_t orc_idmap_build(const int64_t *src, const int64_t *dst, uint64_t n_edges,
+                         uint32_t *dense_src, uint32_t *dense_dst, int64_t *to_user);
 void orc_set_threads(int threads);
 int orc_get_threads(void);
 

@@ -411,3 +411,17 @@ def test_networkx_weak_components(orc, nxg):
     for i, l in enumerate(cc):
         groups.setdefault(int(l), []).append(inv[i])
     assert sorted(sorted(x) for x in groups.values()) == g["weak_components"]
+
+
+def test_idmap_goldens(orc):
+    """IdMap interning, the reference's own cases (id_map.rs:469-575)."""
+    users, sd, dd = orc.idmap_build([10, 10, 20, 30], [20, 30, 30, 10])  # :470-477
+    assert list(users) == [10, 20, 30]
+    assert list(sd) == [0, 0, 1, 2] and list(dd) == [1, 2, 2, 0]
+    # chunks intern like their concatenation (:529-550): the oracle takes
+    # the concatenation, the device path is tested chunk by chunk
+    users, sd, dd = orc.idmap_build([], [])  # :569-573
+    assert users.size == 0 and sd.size == 0 and dd.size == 0
+    # first-seen order over src, dst interleaved (from_ids order, :460-467)
+    users, _, _ = orc.idmap_build([100, 100, 7], [7, 42, 100])
+    assert list(users) == [100, 7, 42]

@@ -169,6 +169,15 @@ SIGNATURES = {
     "ursa_gpu_batch_get_config": (i32, [P, C.POINTER(BatchConfig)]),
     "ursa_gpu_batch_results": (i32, [P, P, P, P, P, P]),
     "ursa_gpu_batch_device_results": (i32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "ursa_gpu_idmap_build": (i32, [u64, P, P, P, C.POINTER(P)]),
+    "ursa_gpu_idmap_free": (None, [P]),
+    "ursa_gpu_idmap_len": (u64, [P]),
+    "ursa_gpu_idmap_n_edges": (u64, [P]),
+    "ursa_gpu_idmap_user_ids": (i32, [P, P]),
+    "ursa_gpu_idmap_dense_edges": (i32, [P, P, P]),
+    "ursa_gpu_idmap_topology": (i32, [P, C.POINTER(P)]),
+    "ursa_gpu_idmap_gather_user": (i32, [P, P, u64, P]),
+    "ursa_gpu_idmap_lookup": (i32, [P, P, u64, P, P]),
     "ursa_gpu_server_create": (i32, [P, C.POINTER(ServerConfig), C.POINTER(P)]),
     "ursa_gpu_server_destroy": (None, [P]),
     "ursa_gpu_server_upload": (i32, [P, u64, P, P, u64, C.POINTER(u32)]),
