@@ -307,6 +307,83 @@ def run_reference_batch(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+IDMAP_WORKLOAD = "idmap_rmat22_int64"
+
+
+def run_idmap(args, rank, world):
+    """Node-id interning (IdMap::from_edge_batches) of the R-MAT-22 edges
+    under seeded random 64-bit user ids, then Topology::build from the dense
+    device columns.  A step: host Int64 columns in (pinned), dense ids and
+    the topology out.  CPU baseline: the oracle's serial restatement."""
+    import torch
+
+    local_rank = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    from ursa_b200 import _lib
+    from ursa_b200.idmap import IdMap
+
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(local_rank))
+    n, s, d = make_workload()
+    m = int(s.size)
+    label = np.random.default_rng(SEED).integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64)
+    h_src = torch.from_numpy(label[s]).pin_memory().numpy()
+    h_dst = torch.from_numpy(label[d]).pin_memory().numpy()
+
+    def step():
+        t0 = time.perf_counter()
+        mp = IdMap.from_edge_arrays(h_src, h_dst)
+        t1 = time.perf_counter()
+        topo = mp.topology()
+        t2 = time.perf_counter()
+        k = len(mp)
+        del topo
+        mp.close()
+        return t1 - t0, t2 - t1, k
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    launches0 = L.ursa_gpu_launch_count()
+    res = [step() for _ in range(args.steps)]
+    launches = L.ursa_gpu_launch_count() - launches0
+    t_map = statistics.median(r[0] for r in res)
+    t_topo = statistics.median(r[1] for r in res)
+    distinct = res[-1][2]
+    line = {
+        "metric": "idmap_edges_per_s",
+        "value": m / t_map,
+        "unit": "edges/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * (t_map + t_topo),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int64 ids -> u32 dense ids",
+        "data": "synthetic",
+        "config": {"workload": IDMAP_WORKLOAD, "n_edges": m, "distinct_ids": distinct,
+                   "ids": "seeded uniform random int64 per R-MAT-22 node"},
+        "e2e": {"value": m / (t_map + t_topo), "unit": "edges/s", "h2d_bytes_per_step": 16 * m,
+                "d2h_bytes_per_step": 0, "ms_per_step": 1e3 * (t_map + t_topo),
+                "note": "host Int64 columns to a resident Topology (interning + CSR build + transpose)"},
+        "idmap_ms": 1e3 * t_map, "topology_ms": 1e3 * t_topo,
+        "gpu_launches": int(launches),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        O.build()
+        k = min(m, 8_000_000)
+        t0 = time.perf_counter()
+        O.idmap_build(h_src[:k], h_dst[:k])
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / dt, "unit": "edges/s", "cores": 1, "kind": "port",
+                                "sample": f"serial interning of the first {k:,} edges (the reference interns serially)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 SERVE_WORKLOAD = "serve_rmat24_uploads"
 SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
 
@@ -700,7 +777,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve"])
+    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids (defaults give the benchmark above)
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="pagerank max_iter (rmat22 workload)")
@@ -727,6 +804,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, rank, world)
+        return
+    if args.workload == "idmap":
+        run_idmap(args, rank, world)
         return
 
     import torch
