@@ -215,6 +215,25 @@ int ursa_gpu_betweenness_weighted(ursa_gpu_topo *t, const double *weights, uint6
                                   int has_sample, double sample, int has_seed, uint64_t seed,
                                   double *out);
 
+/* closeness(&Topology) -> Vec<f64> -- algo/closeness.rs:69-135: per node,
+ * reachable / sum of hop distances over the nodes it reaches (out-edges),
+ * 0.0 if it reaches none.  A bit-parallel BFS from 64 sources at a time;
+ * exact integer folds, so bit-identical to the reference. */
+int ursa_gpu_closeness(ursa_gpu_topo *t, double *out);
+/* closeness_weighted(&Topology, &[f64]) -> Vec<f64> -- algo/closeness.rs:
+ * 137-224: Dijkstra distances per source (exact), summed in node order. */
+int ursa_gpu_closeness_weighted(ursa_gpu_topo *t, const double *weights, uint64_t n_weights,
+                                double *out);
+/* avg_path_length(&Topology, Option<f64>) -- ursa-plan/src/stats.rs:142-150:
+ * mean hop distance over reachable ordered pairs from all sources (or the
+ * deterministic strided sample, stats.rs:82-101); 0.0 with no pair.
+ * URSA_GPU_EINVAL if the distance total reaches 2^53. */
+int ursa_gpu_avg_path_length(ursa_gpu_topo *t, int has_sample, double sample, double *out);
+/* diameter(&Topology, bool approximate) -- stats.rs:152-167: the largest
+ * finite hop distance over all sources (or a strided sample of min(128, n)
+ * sources when approximate). */
+int ursa_gpu_diameter(ursa_gpu_topo *t, int approximate, int64_t *out);
+
 /* ------------------------------------------------------------------------
  * Node-id interning on the device.
  *

@@ -73,6 +73,12 @@ def lib():
         L.orc_sample_indices.argtypes = [u64, u64, i32, u64, P]
         L.orc_sample_sources.restype = u64
         L.orc_sample_sources.argtypes = [u64, i32, f64, i32, u64, P]
+        L.orc_closeness.argtypes = [P, P]
+        L.orc_closeness_weighted.argtypes = [P, P, P]
+        L.orc_avg_path_length.restype = f64
+        L.orc_avg_path_length.argtypes = [P, i32, f64]
+        L.orc_diameter.restype = i64
+        L.orc_diameter.argtypes = [P, i32]
         L.orc_idmap_build.restype = u64
         L.orc_idmap_build.argtypes = [P, P, u64, P, P, P]
         L.orc_set_threads.argtypes = [i32]
@@ -280,3 +286,28 @@ def idmap_build(src, dst):
     users = np.empty(2 * s.size, np.int64)
     k = lib().orc_idmap_build(_p(s), _p(d), s.size, _p(ds), _p(dd), _p(users))
     return users[:k].copy(), ds, dd
+
+
+def closeness(t: Topology) -> np.ndarray:
+    """closeness (ursa-core/src/algo/closeness.rs:69-135)."""
+    out = np.empty(t.n, np.float64)
+    lib().orc_closeness(t._h, _p(out))
+    return out
+
+
+def closeness_weighted(t: Topology, weights) -> np.ndarray:
+    """closeness_weighted (ursa-core/src/algo/closeness.rs:137-224)."""
+    w = _f64(weights)
+    out = np.empty(t.n, np.float64)
+    lib().orc_closeness_weighted(t._h, _p(w), _p(out))
+    return out
+
+
+def avg_path_length(t: Topology, sample=None) -> float:
+    """avg_path_length (ursa-plan/src/stats.rs:142-150)."""
+    return float(lib().orc_avg_path_length(t._h, int(sample is not None), float(sample or 0.0)))
+
+
+def diameter(t: Topology, approximate: bool = True) -> int:
+    """diameter (ursa-plan/src/stats.rs:152-167)."""
+    return int(lib().orc_diameter(t._h, int(bool(approximate))))

@@ -1413,3 +1413,143 @@ uint64_t orc_idmap_build(const int64_t *src, const int64_t *dst, uint64_t n_edge
   free(used);
   return next;
 }
+
+/* ------------------------------------------------------------------------ */
+/* closeness / closeness_weighted (algo/closeness.rs:69-224) and the path     */
+/* statistics avg_path_length / diameter (ursa-plan/src/stats.rs:82-167).     */
+/* Each source's traversal is independent: sources run in parallel ranges,   */
+/* each writing its own slots; folds across sources happen in source order.   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  orc_topo *t;
+  const double *w;
+  const uint32_t *sources;
+  double *out;          /* closeness per source */
+  int64_t *sum, *cnt;   /* per-source hop-distance folds (stats) */
+  int32_t *mx;
+} clo_ctx;
+
+static void clo_range(void *p, uint64_t lo, uint64_t hi, int tid) {
+  (void)tid;
+  clo_ctx *c = (clo_ctx *)p;
+  uint64_t n = c->t->n;
+  int32_t *dist = (int32_t *)malloc((n ? n : 1) * sizeof(int32_t));
+  for (uint64_t i = lo; i < hi; i++) {
+    uint32_t u = c->sources ? c->sources[i] : (uint32_t)i;
+    orc_bfs_distances(c->t, u, 0, dist);
+    int64_t sum = 0, reach = 0;
+    int32_t mx = 0;
+    for (uint64_t v = 0; v < n; v++)
+      if (dist[v] >= 1) { /* closeness.rs:115-122, stats.rs:112-121 */
+        sum += dist[v];
+        reach++;
+        if (dist[v] > mx) mx = dist[v];
+      }
+    if (c->out) c->out[i] = sum > 0 ? (double)reach / (double)sum : 0.0;
+    if (c->sum) {
+      c->sum[i] = sum;
+      c->cnt[i] = reach;
+      c->mx[i] = mx;
+    }
+  }
+  free(dist);
+}
+
+void orc_closeness(orc_topo *t, double *out) {
+  clo_ctx c = {t, NULL, NULL, out, NULL, NULL, NULL};
+  par_ranges(t->n, par_threads_for(t->n * (t->n + t->m)), clo_range, &c);
+}
+
+static void clow_range(void *p, uint64_t lo, uint64_t hi, int tid) {
+  (void)tid;
+  clo_ctx *c = (clo_ctx *)p;
+  uint64_t n = c->t->n;
+  double *dist = (double *)malloc((n ? n : 1) * sizeof(double));
+  for (uint64_t u = lo; u < hi; u++) {
+    orc_dijkstra_distances(c->t, c->w, (uint32_t)u, 0, dist);
+    double sum = 0.0; /* node-order fold (closeness.rs:196-217) */
+    int64_t reach = 0;
+    for (uint64_t v = 0; v < n; v++)
+      if (v != u && isfinite(dist[v])) {
+        sum += dist[v];
+        reach++;
+      }
+    c->out[u] = sum > 0.0 ? (double)reach / sum : 0.0;
+  }
+  free(dist);
+}
+
+void orc_closeness_weighted(orc_topo *t, const double *w, double *out) {
+  clo_ctx c = {t, w, NULL, out, NULL, NULL, NULL};
+  par_ranges(t->n, par_threads_for(t->n * (t->n + t->m)), clow_range, &c);
+}
+
+/* stats.rs:82-101 sample_sources: None -> all; Some(frac) -> k evenly strided. */
+static uint64_t stats_sources(uint64_t n, int has_frac, double frac, uint32_t *out) {
+  if (!has_frac) {
+    for (uint64_t i = 0; i < n; i++) out[i] = (uint32_t)i;
+    return n;
+  }
+  double f = frac < 0.0 ? 0.0 : (frac > 1.0 ? 1.0 : frac);
+  double kd = round((double)n * f);
+  if (kd < 1.0) kd = 1.0;
+  uint64_t k = (uint64_t)kd;
+  if (k > n) k = n;
+  double step = k ? (double)n / (double)k : 1.0;
+  if (step < 1.0) step = 1.0;
+  for (uint64_t i = 0; i < k; i++) {
+    uint64_t v = (uint64_t)floor((double)i * step);
+    out[i] = (uint32_t)(v < n - 1 ? v : n - 1);
+  }
+  return k;
+}
+
+/* bfs_source_scan (stats.rs:107-140): per-source f64 sums folded in source
+ * order. */
+static void stats_scan(orc_topo *t, const uint32_t *src, uint64_t k, double *sum, uint64_t *count,
+                       int32_t *max) {
+  int64_t *ps = (int64_t *)malloc((k ? k : 1) * sizeof(int64_t));
+  int64_t *pc = (int64_t *)malloc((k ? k : 1) * sizeof(int64_t));
+  int32_t *pm = (int32_t *)malloc((k ? k : 1) * sizeof(int32_t));
+  clo_ctx c = {t, NULL, src, NULL, ps, pc, pm};
+  par_ranges(k, par_threads_for(k * (t->n + t->m)), clo_range, &c);
+  double s = 0.0;
+  uint64_t cnt = 0;
+  int32_t mx = 0;
+  for (uint64_t i = 0; i < k; i++) {
+    s += (double)ps[i]; /* a per-source f64 sum of integers: exact below 2^53 */
+    cnt += (uint64_t)pc[i];
+    if (pm[i] > mx) mx = pm[i];
+  }
+  *sum = s;
+  *count = cnt;
+  *max = mx;
+  free(ps);
+  free(pc);
+  free(pm);
+}
+
+double orc_avg_path_length(orc_topo *t, int has_sample, double sample) {
+  uint32_t *src = (uint32_t *)malloc((t->n ? t->n : 1) * sizeof(uint32_t));
+  uint64_t k = stats_sources(t->n, has_sample, sample, src);
+  double sum;
+  uint64_t count;
+  int32_t mx;
+  stats_scan(t, src, k, &sum, &count, &mx);
+  free(src);
+  return count == 0 ? 0.0 : sum / (double)count;
+}
+
+int64_t orc_diameter(orc_topo *t, int approximate) {
+  uint64_t n = t->n;
+  uint32_t *src = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+  uint64_t k = approximate && n > 0
+                   ? stats_sources(n, 1, fmin(128.0 / (double)n, 1.0), src)
+                   : stats_sources(n, 0, 0.0, src);
+  double sum;
+  uint64_t count;
+  int32_t mx;
+  stats_scan(t, src, k, &sum, &count, &mx);
+  free(src);
+  return mx;
+}

@@ -30,6 +30,12 @@ typedef struct orc_topo orc_topo;
  * to 2 * n_edges ids; returns the number of distinct ids. */
 uint64_t orc_idmap_build(const int64_t *src, const int64_t *dst, uint64_t n_edges,
                          uint32_t *dense_src, uint32_t *dense_dst, int64_t *to_user);
+/* closeness / closeness_weighted (algo/closeness.rs:69-224) and
+ * avg_path_length / diameter (ursa-plan/src/stats.rs:82-167). */
+void orc_closeness(orc_topo *t, double *out);
+void orc_closeness_weighted(orc_topo *t, const double *weights, double *out);
+double orc_avg_path_length(orc_topo *t, int has_sample, double sample);
+int64_t orc_diameter(orc_topo *t, int approximate);
 void orc_set_threads(int threads);
 int orc_get_threads(void);
 

@@ -1,0 +1,81 @@
+"""Closeness and the path statistics on the device vs the oracle
+(ursa-core/src/algo/closeness.rs:69-224, ursa-plan/src/stats.rs:82-167).
+
+Bit-exact: unweighted closeness (integer folds, one f64 division per node),
+avg_path_length and diameter (integer distance totals below 2^53), and
+weighted closeness (exact Dijkstra distances, node-order f64 sums).
+"""
+
+import numpy as np
+import pytest
+
+from cases import random_graph, small_cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.asarray(a, np.float64).view(np.uint64)
+
+
+def _cases():
+    from ursa_b200 import gen
+
+    out = [(name, n, s, d) for name, n, s, d in small_cases()]
+    out.append(("rand_300", *random_graph(300, 1200, 4)))
+    out.append(("rand_2000", *random_graph(2000, 6000, 5)))  # more than 64 sources per batch
+    n, s, d = gen.rmat(11, 8, 9)
+    out.append(("rmat11", n, s, d))
+    chain = 130
+    out.append(("chain130", chain, list(range(chain - 1)), list(range(1, chain))))  # 129 levels
+    return out
+
+
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: c[0])
+def test_closeness_exact(orc, case):
+    from ursa_b200 import Topology, algo
+
+    _, n, s, d = case
+    got = algo.closeness(Topology.build(n, s, d))
+    ref = orc.closeness(orc.Topology(n, s, d))
+    assert np.array_equal(_bits(got), _bits(ref))
+
+
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: c[0])
+def test_path_stats_exact(orc, case):
+    from ursa_b200 import Topology, algo
+
+    _, n, s, d = case
+    g, o = Topology.build(n, s, d), orc.Topology(n, s, d)
+    for sample in (None, 0.1, 0.5, 1.0):
+        assert _bits([algo.avg_path_length(g, sample)])[0] == _bits([orc.avg_path_length(o, sample)])[0], sample
+    for approx in (False, True):
+        assert algo.diameter(g, approx) == orc.diameter(o, approx)
+
+
+@pytest.mark.parametrize("case", [c for c in _cases() if c[1] <= 400], ids=lambda c: c[0])
+def test_closeness_weighted_exact(orc, case):
+    from ursa_b200 import Topology, algo
+
+    _, n, s, d = case
+    rng = np.random.default_rng(n)
+    w = rng.uniform(0.0, 4.0, len(s))
+    if len(w):
+        w[rng.integers(0, len(w), max(1, len(w) // 10))] = 0.0  # zero-cost edges
+    got = algo.closeness_weighted(Topology.build(n, s, d), w)
+    ref = orc.closeness_weighted(orc.Topology(n, s, d), w)
+    assert np.array_equal(_bits(got), _bits(ref))
+
+
+def test_reference_goldens():
+    from ursa_b200 import Topology, algo
+
+    c = algo.closeness(Topology.build(4, [0, 1, 2], [1, 2, 3]))
+    assert list(c) == [0.5, 2.0 / 3.0, 1.0, 0.0]  # closeness.rs directed line
+    assert algo.closeness(Topology.build(0, [], [])).size == 0
+    c = algo.closeness_weighted(Topology.build(3, [0, 1, 0], [1, 2, 2]), [1.0, 1.0, 5.0])
+    assert abs(c[0] - 2.0 / 3.0) < 1e-12 and abs(c[1] - 1.0) < 1e-12
+    tri = Topology.build(3, [0, 1, 2], [1, 2, 0])
+    assert algo.avg_path_length(tri) == 1.5 and algo.diameter(tri, False) == 2  # stats.rs
+    two = Topology.build(4, [0, 2], [1, 3])
+    assert algo.avg_path_length(two) == 1.0 and algo.diameter(two, False) == 1

@@ -425,3 +425,32 @@ def test_idmap_goldens(orc):
     # first-seen order over src, dst interleaved (from_ids order, :460-467)
     users, _, _ = orc.idmap_build([100, 100, 7], [7, 42, 100])
     assert list(users) == [100, 7, 42]
+
+
+def test_closeness_goldens(orc):
+    """algo/closeness.rs tests."""
+    T = orc.Topology
+    c = orc.closeness(T(3, [0, 1, 2], [1, 2, 0]))  # directed triangle
+    assert all(abs(x - 2.0 / 3.0) < 1e-12 for x in c)
+    c = orc.closeness(T(4, [0, 1, 2], [1, 2, 3]))  # directed line
+    assert abs(c[0] - 0.5) < 1e-12 and abs(c[1] - 2.0 / 3.0) < 1e-12 and abs(c[2] - 1.0) < 1e-12 and c[3] == 0.0
+    assert orc.closeness(T(0, [], [])).size == 0
+    c = orc.closeness(T(100, list(range(100)), [(i + 1) % 100 for i in range(100)]))
+    assert all(abs(x - c[0]) < 1e-12 for x in c) and c[0] > 0.0
+    c = orc.closeness_weighted(T(3, [0, 1, 0], [1, 2, 2]), [1.0, 1.0, 5.0])
+    assert abs(c[0] - 2.0 / 3.0) < 1e-12 and abs(c[1] - 1.0) < 1e-12
+    c = orc.closeness_weighted(T(3, [0, 1], [1, 2]), [0.0, 1.0])  # zero-weight reachable node counted
+    assert abs(c[0] - 2.0) < 1e-12 and abs(c[1] - 1.0) < 1e-12
+    c = orc.closeness_weighted(T(3, [0, 0], [1, 2]), [0.0, 0.0])
+    assert c[0] == 0.0
+
+
+def test_path_stats_goldens(orc):
+    """ursa-plan/src/stats.rs tests."""
+    T = orc.Topology
+    tri = T(3, [0, 1, 2], [1, 2, 0])
+    assert abs(orc.avg_path_length(tri) - 1.5) < 1e-12
+    assert orc.diameter(tri, False) == 2 and orc.diameter(tri, True) <= 2
+    assert orc.diameter(T(4, [0, 1, 2], [1, 2, 3]), False) == 3
+    two = T(4, [0, 2], [1, 3])
+    assert abs(orc.avg_path_length(two) - 1.0) < 1e-12 and orc.diameter(two, False) == 1

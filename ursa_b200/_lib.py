@@ -169,6 +169,10 @@ SIGNATURES = {
     "ursa_gpu_batch_get_config": (i32, [P, C.POINTER(BatchConfig)]),
     "ursa_gpu_batch_results": (i32, [P, P, P, P, P, P]),
     "ursa_gpu_batch_device_results": (i32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "ursa_gpu_closeness": (i32, [P, P]),
+    "ursa_gpu_closeness_weighted": (i32, [P, P, u64, P]),
+    "ursa_gpu_avg_path_length": (i32, [P, i32, f64, C.POINTER(f64)]),
+    "ursa_gpu_diameter": (i32, [P, i32, C.POINTER(i64)]),
     "ursa_gpu_idmap_build": (i32, [u64, P, P, P, C.POINTER(P)]),
     "ursa_gpu_idmap_free": (None, [P]),
     "ursa_gpu_idmap_len": (u64, [P]),

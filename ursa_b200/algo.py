@@ -176,3 +176,33 @@ def betweenness_weighted(topo: Topology, weights, sample: float | None = None, s
                                                           float(sample or 0.0), seed is not None, int(seed or 0),
                                                           out.ctypes.data))
     return out
+
+
+def closeness(topo: Topology) -> np.ndarray:
+    """closeness (algo/closeness.rs:69-135)."""
+    out = np.empty(topo.n_nodes(), np.float64)
+    _lib.check(_lib.load().ursa_gpu_closeness(topo.handle, out.ctypes.data))
+    return out
+
+
+def closeness_weighted(topo: Topology, weights) -> np.ndarray:
+    """closeness_weighted (algo/closeness.rs:137-224)."""
+    w = _f64(weights)
+    out = np.empty(topo.n_nodes(), np.float64)
+    _lib.check(_lib.load().ursa_gpu_closeness_weighted(topo.handle, w.ctypes.data, w.size, out.ctypes.data))
+    return out
+
+
+def avg_path_length(topo: Topology, sample=None) -> float:
+    """avg_path_length (ursa-plan/src/stats.rs:142-150)."""
+    out = C.c_double()
+    _lib.check(_lib.load().ursa_gpu_avg_path_length(topo.handle, int(sample is not None),
+                                                     float(sample or 0.0), C.byref(out)))
+    return out.value
+
+
+def diameter(topo: Topology, approximate: bool = True) -> int:
+    """diameter (ursa-plan/src/stats.rs:152-167)."""
+    out = C.c_int64()
+    _lib.check(_lib.load().ursa_gpu_diameter(topo.handle, int(bool(approximate)), C.byref(out)))
+    return out.value
