@@ -3,18 +3,28 @@
 // avg_path_length / diameter (ursa-plan/src/stats.rs:82-170).
 //
 // Sources are taken 64 at a time; bit b of a node's 64-bit masks belongs to
-// source b of the batch.  Per BFS level (following out-edges):
-//   pull:  next[w] |= frontier[v] & ~visited[w] for every in-edge v -> w
-//          (edge-parallel over the in-CSR, 64-bit atomicOr);
-//   settle: new = next[w] & ~visited[w]; visited |= new; frontier = new;
-//          per source, the number of nodes first reached on this level is a
-//          column popcount of the new masks (one warp ballot per bit);
-//   fold:  reach[b] += count[b]; dist_sum[b] += level * count[b];
-//          max_dist[b] = level where count[b] > 0.
+// source b of the batch.  One persistent cooperative kernel runs a group of
+// batches; each BFS level (following out-edges) ends in a bounded grid
+// barrier and goes one of two ways (direction-optimising BFS):
+//   top-down while the frontier's out-edges are below m / 8: each frontier
+//   node ORs its mask into acc[w] for out-edges v -> w whose target lacks some
+//   of its sources; after a barrier every w settles new = acc[w] & ~visited[w];
+//   bottom-up otherwise: each w with sources still to find
+//   (need = active & ~visited[w]) ORs its in-neighbours' frontier masks,
+//   stopping as soon as every needed bit is found; new = acc & need.
+//   Nodes with at most 32 edges to scan are handled by one lane, heavier ones
+//   by the whole warp.  visited[w] |= new; next[w] = new.
+// A source that reached no new node on a level is finished and leaves the
+// active mask.  Per source, the number of nodes first reached on the level is
+// a column popcount of the new masks (one warp ballot per bit), summed per
+// block in shared memory and per grid in a level-indexed counter row, which
+// also carries the new frontier's out-edge count for the next direction.
+// Block 0 folds the counts after the barrier: reach[b] += count[b];
+// dist_sum[b] += level * count[b]; max_dist[b] = level where count[b] > 0.
 // The folds are integer and exact, so the reference's results follow
 // bit-for-bit: closeness = reach / sum (an i64 sum in closeness_one), and the
 // stats' f64 sums of integer distances are exact while the total stays below
-// 2^53 (checked).  Costs O(n / 64 * levels * (m + n)).
+// 2^53 (checked).  A level with no new node ends the batch.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -29,78 +39,231 @@ void dijkstra_run(TopoImpl* t, const double* d_weights, uint32_t source, int dir
 
 namespace {
 
-__global__ void ms_init_k(const uint32_t* __restrict__ src, uint32_t k, unsigned long long* visited,
-                          unsigned long long* frontier) {
-  const uint32_t b = threadIdx.x;
-  if (b < k) {
-    atomicOr(&visited[src[b]], 1ull << b);
-    atomicOr(&frontier[src[b]], 1ull << b);
+constexpr int kMsBlock = 256;
+constexpr int kMsWarps = kMsBlock / 32;
+constexpr uint64_t kMsBatchesPerLaunch = 16;
+constexpr uint64_t kMsWaitNs = 5000000000ull;  // one grid-barrier wait
+constexpr int kMsRow = 72;  // per-level counter row: 64 per-source counts, [64] = frontier out-edges
+constexpr uint64_t kMsPushDiv = 8;  // push while the frontier's out-edges are below m / 8
+
+struct MsArgs {
+  const uint32_t* in_off;
+  const uint32_t* in_src;
+  const uint32_t* out_off;
+  const uint32_t* out_tgt;
+  uint64_t n, m;
+  const uint32_t* sources;  // n_sources ids < n
+  uint64_t n_sources;
+  uint64_t b_begin, b_end;  // batches of 64 sources run by this launch
+  unsigned long long* visited;
+  unsigned long long* fr0;    // frontier masks, odd levels' input
+  unsigned long long* fr1;    // even levels' input
+  unsigned long long* acc;    // pushed masks of a top-down level; all zero between levels
+  unsigned long long* count;  // 3 rows of kMsRow, row = level % 3
+  unsigned long long* reach;
+  unsigned long long* dsum;
+  uint32_t* maxd;
+  unsigned* bar;  // grid barrier count, generation
+  int* err;
+};
+
+__device__ __forceinline__ unsigned long long warp_or64(unsigned long long v) {
+  const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)v);
+  const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(v >> 32));
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+// Top-down half of a level: every frontier node v ORs its mask into acc[w]
+// for each out-edge v -> w whose target still lacks some of those sources.
+__device__ __forceinline__ void ms_push(const MsArgs& a, const unsigned long long* cur, uint64_t gwarp,
+                                        uint64_t nwarps, int lane) {
+  for (uint64_t c0 = gwarp * 32; c0 < a.n; c0 += nwarps * 32) {
+    const uint64_t v = c0 + lane;
+    unsigned long long f = 0;
+    uint32_t e0 = 0, e1 = 0;
+    if (v < a.n) {
+      f = __ldcg(&cur[v]);
+      if (f) {
+        e0 = __ldg(&a.out_off[v]);
+        e1 = __ldg(&a.out_off[v + 1]);
+      }
+    }
+    const bool heavy = f && e1 - e0 > 32;
+    if (f && !heavy) {
+      for (uint32_t e = e0; e < e1; e++) {
+        const uint32_t w = __ldg(&a.out_tgt[e]);
+        const unsigned long long add = f & ~__ldcg(&a.visited[w]);
+        if (add) atomicOr(&a.acc[w], add);
+      }
+    }
+    unsigned hm = __ballot_sync(0xffffffffu, heavy);
+    while (hm) {
+      const int j = __ffs(hm) - 1;
+      hm &= hm - 1;
+      const uint32_t h0 = __shfl_sync(0xffffffffu, e0, j), h1 = __shfl_sync(0xffffffffu, e1, j);
+      const unsigned long long hf = __shfl_sync(0xffffffffu, f, j);
+      for (uint32_t e = h0 + lane; e < h1; e += 32) {
+        const uint32_t w = __ldg(&a.out_tgt[e]);
+        const unsigned long long add = hf & ~__ldcg(&a.visited[w]);
+        if (add) atomicOr(&a.acc[w], add);
+      }
+    }
   }
 }
 
-// next[w] |= frontier[v] & ~visited[w] over the in-edges v -> w of w.
-__global__ void ms_pull_k(const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src,
-                          uint64_t n, uint64_t m, const unsigned long long* __restrict__ frontier,
-                          const unsigned long long* __restrict__ visited, unsigned long long* next) {
-  for_each_slot_owner(in_off, n, m, [&](uint64_t k, uint32_t w) {
-    const unsigned long long f = frontier[in_src[k]];
-    if (f) {
-      const unsigned long long add = f & ~visited[w];
-      if (add) atomicOr(&next[w], add);
-    }
-  });
-}
-
-// Settles the level and counts, per source bit, the nodes first reached.
-__global__ void ms_settle_k(uint64_t n, unsigned long long* __restrict__ visited,
-                            unsigned long long* __restrict__ frontier,
-                            unsigned long long* __restrict__ next,
-                            unsigned long long* __restrict__ count) {
-  __shared__ unsigned int sc[64];
-  if (threadIdx.x < 64) sc[threadIdx.x] = 0;
-  __syncthreads();
+__global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
+  __shared__ unsigned sc[64];
+  __shared__ unsigned long long s_mf;
+  __shared__ unsigned s_act[2];
   const int lane = threadIdx.x & 31;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n;
-       base += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t w = base + threadIdx.x;
-    unsigned long long nw = 0;
-    if (w < n) {
-      const unsigned long long nx = next[w];
-      if (nx) {
-        nw = nx & ~visited[w];
-        visited[w] |= nw;
-        next[w] = 0;
-      }
-      frontier[w] = nw;
+  const uint64_t n = a.n;
+  const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
+  const uint64_t gwarp = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t bt = a.b_begin; bt < a.b_end; bt++) {
+    const uint64_t s0 = bt * 64;
+    const uint64_t left = a.n_sources - s0;
+    const uint32_t k = left < 64 ? (uint32_t)left : 64u;
+    const unsigned long long full = k == 64 ? ~0ull : ((1ull << k) - 1);
+    for (uint64_t w = gtid; w < n; w += nthreads) {
+      a.visited[w] = 0;
+      a.fr0[w] = 0;
     }
-    if (__any_sync(0xffffffffu, nw != 0)) {
-      // column popcount: bit b of the 32 lanes' masks
+    grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+    if (*(volatile int*)a.err) return;
+    if (blockIdx.x == 0) {  // every block has read the previous batch's last counter row
+      if (threadIdx.x < 3 * kMsRow) a.count[threadIdx.x] = 0;
+      __syncthreads();
+      if (threadIdx.x < k) {
+        const uint32_t src = a.sources[s0 + threadIdx.x];
+        atomicOr(&a.visited[src], 1ull << threadIdx.x);
+        atomicOr(&a.fr0[src], 1ull << threadIdx.x);
+        atomicAdd(&a.count[64], (unsigned long long)(a.out_off[src + 1] - a.out_off[src]));
+      }
+    }
+    grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+    if (*(volatile int*)a.err) return;
+    unsigned long long reach = 0, dsum = 0;  // block 0, thread b < k: source s0 + b
+    uint32_t maxd = 0;
+    unsigned long long active = full;  // sources whose search still grows
+    for (uint32_t level = 1;; level++) {
+      const unsigned long long* cur = (level & 1) ? a.fr0 : a.fr1;
+      unsigned long long* nxt = (level & 1) ? a.fr1 : a.fr0;
+      unsigned long long* row = a.count + (level % 3) * kMsRow;
+      const unsigned long long mf = __ldcg(&a.count[((level - 1) % 3) * kMsRow + 64]);
+      const bool push = mf * kMsPushDiv < a.m;
+      if (threadIdx.x < 64) sc[threadIdx.x] = 0;
+      if (threadIdx.x == 0) s_mf = 0;
+      // row (level + 1) % 3 was last read before the previous barrier
+      if (blockIdx.x == 0 && threadIdx.x < kMsRow) a.count[((level + 1) % 3) * kMsRow + threadIdx.x] = 0;
+      __syncthreads();
+      if (push) {
+        ms_push(a, cur, gwarp, nwarps, lane);
+        grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+        if (*(volatile int*)a.err) return;
+      }
+      for (uint64_t c0 = gwarp * 32; c0 < n; c0 += nwarps * 32) {
+        const uint64_t w = c0 + lane;
+        unsigned long long vis = 0, nw = 0;
+        if (push) {
+          if (w < n) {
+            const unsigned long long p = __ldcg(&a.acc[w]);
+            if (p) {
+              a.acc[w] = 0;
+              vis = __ldcg(&a.visited[w]);
+              nw = p & ~vis;
+            }
+          }
+        } else {
+          // bottom-up: OR the in-neighbours' frontier masks until every
+          // needed source is found
+          unsigned long long need = 0, acc = 0;
+          uint32_t e0 = 0, e1 = 0;
+          if (w < n) {
+            vis = __ldcg(&a.visited[w]);
+            need = active & ~vis;
+            if (need) {
+              e0 = __ldg(&a.in_off[w]);
+              e1 = __ldg(&a.in_off[w + 1]);
+            }
+          }
+          const bool heavy = need && e1 - e0 > 32;
+          if (need && !heavy) {
+            for (uint32_t e = e0; e < e1; e += 4) {
+              const uint32_t r = e1 - e;
+              const uint32_t v0 = __ldg(&a.in_src[e]);
+              const uint32_t v1 = r > 1 ? __ldg(&a.in_src[e + 1]) : v0;
+              const uint32_t v2 = r > 2 ? __ldg(&a.in_src[e + 2]) : v0;
+              const uint32_t v3 = r > 3 ? __ldg(&a.in_src[e + 3]) : v0;
+              acc |= __ldcg(&cur[v0]) | __ldcg(&cur[v1]) | __ldcg(&cur[v2]) | __ldcg(&cur[v3]);
+              if ((acc & need) == need) break;
+            }
+          }
+          unsigned hm = __ballot_sync(0xffffffffu, heavy);
+          while (hm) {
+            const int j = __ffs(hm) - 1;
+            hm &= hm - 1;
+            const uint32_t h0 = __shfl_sync(0xffffffffu, e0, j), h1 = __shfl_sync(0xffffffffu, e1, j);
+            const unsigned long long hneed = __shfl_sync(0xffffffffu, need, j);
+            unsigned long long hacc = 0;
+            for (uint32_t e = h0; e < h1; e += 128) {
+              unsigned long long f = 0;
+#pragma unroll
+              for (int q = 0; q < 4; q++) {
+                const uint32_t x = e + q * 32 + lane;
+                if (x < h1) f |= __ldcg(&cur[__ldg(&a.in_src[x])]);
+              }
+              hacc |= warp_or64(f);
+              if ((hacc & hneed) == hneed) break;
+            }
+            if (lane == j) acc = hacc;
+          }
+          nw = acc & need;
+        }
+        unsigned long long od = 0;
+        if (w < n) {
+          if (nw) {
+            a.visited[w] = vis | nw;
+            od = __ldg(&a.out_off[w + 1]) - __ldg(&a.out_off[w]);
+          }
+          nxt[w] = nw;
+        }
+        if (__any_sync(0xffffffffu, nw != 0)) {
 #pragma unroll 8
-      for (int b = 0; b < 64; b++) {
-        const unsigned c = __popc(__ballot_sync(0xffffffffu, (nw >> b) & 1ull));
-        if (lane == 0 && c) atomicAdd(&sc[b], c);
+          for (int b = 0; b < 64; b++) {
+            const unsigned c = __popc(__ballot_sync(0xffffffffu, (nw >> b) & 1ull));
+            if (lane == 0 && c) atomicAdd(&sc[b], c);
+          }
+          for (int o = 16; o; o >>= 1) od += __shfl_down_sync(0xffffffffu, od, o);
+          if (lane == 0) atomicAdd(&s_mf, od);
+        }
       }
+      __syncthreads();
+      if (threadIdx.x < 64 && sc[threadIdx.x])
+        atomicAdd(&row[threadIdx.x], (unsigned long long)sc[threadIdx.x]);
+      if (threadIdx.x == 0 && s_mf) atomicAdd(&row[64], s_mf);
+      grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+      if (*(volatile int*)a.err) return;
+      unsigned long long c = 0;
+      if (threadIdx.x < 64) c = __ldcg(&row[threadIdx.x]);
+      if (blockIdx.x == 0 && c) {  // only bits < k are ever counted
+        reach += c;
+        dsum += (unsigned long long)level * c;
+        maxd = level;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, c != 0);
+      if (threadIdx.x == 0) s_act[0] = bal;
+      if (threadIdx.x == 32) s_act[1] = bal;
+      __syncthreads();
+      // a source that reached nobody new on this level is finished
+      active = ((unsigned long long)s_act[1] << 32) | s_act[0];
+      if (!active) break;
     }
-  }
-  __syncthreads();
-  if (threadIdx.x < 64 && sc[threadIdx.x]) atomicAdd(&count[threadIdx.x], (unsigned long long)sc[threadIdx.x]);
-}
-
-// Folds one level's counts into the per-source results and reports whether
-// any node was reached.
-__global__ void ms_fold_k(uint32_t level, uint32_t k, unsigned long long* __restrict__ count,
-                          unsigned long long* __restrict__ reach,
-                          unsigned long long* __restrict__ dsum, uint32_t* __restrict__ maxd,
-                          unsigned* __restrict__ any) {
-  const uint32_t b = threadIdx.x;
-  if (b < 64) {
-    const unsigned long long c = count[b];
-    count[b] = 0;
-    if (b < k && c) {
-      reach[b] += c;
-      dsum[b] += (unsigned long long)level * c;
-      maxd[b] = level;
-      atomicOr(any, 1u);
+    if (blockIdx.x == 0 && threadIdx.x < k) {
+      a.reach[s0 + threadIdx.x] = reach;
+      a.dsum[s0 + threadIdx.x] = dsum;
+      a.maxd[s0 + threadIdx.x] = maxd;
     }
   }
 }
@@ -112,45 +275,54 @@ __global__ void ms_fold_k(uint32_t level, uint32_t k, unsigned long long* __rest
 // out-edges.  Outputs are host arrays of n_sources entries.
 void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_t* reach,
                uint64_t* dsum, uint32_t* maxd, cudaStream_t s) {
-  const uint64_t n = t->n, m = t->m;
+  const uint64_t n = t->n;
   if (n_sources == 0) return;
   ensure_in(t, s);
-  Scratch<unsigned long long> visited(n, s), frontier(n, s), next(n, s);
-  Scratch<unsigned long long> count(64, s), d_reach(64, s), d_dsum(64, s);
-  Scratch<uint32_t> d_maxd(64, s), d_src(64, s);
-  Scratch<unsigned> any(1, s);
-  UG_CUDA(cudaMemsetAsync(next.get(), 0, n * 8, s));
-  UG_CUDA(cudaMemsetAsync(count.get(), 0, 64 * 8, s));
-  for (uint64_t b0 = 0; b0 < n_sources; b0 += 64) {
-    const uint32_t k = (uint32_t)std::min<uint64_t>(64, n_sources - b0);
-    UG_CUDA(cudaMemsetAsync(visited.get(), 0, n * 8, s));
-    UG_CUDA(cudaMemsetAsync(frontier.get(), 0, n * 8, s));
-    UG_CUDA(cudaMemsetAsync(d_reach.get(), 0, 64 * 8, s));
-    UG_CUDA(cudaMemsetAsync(d_dsum.get(), 0, 64 * 8, s));
-    UG_CUDA(cudaMemsetAsync(d_maxd.get(), 0, 64 * 4, s));
-    UG_CUDA(cudaMemcpyAsync(d_src.get(), sources + b0, k * 4, cudaMemcpyHostToDevice, s));
-    ms_init_k<<<1, 64, 0, s>>>(d_src.get(), k, visited.get(), frontier.get());
-    UG_LAUNCH_CHECK();
-    for (uint32_t level = 1;; level++) {
-      if (m) {
-        ms_pull_k<<<grid_for(m, kBlock, 148u * 64u), kBlock, 0, s>>>(
-            t->in.off.get(), t->in.tgt.get(), n, m, frontier.get(), visited.get(), next.get());
-        UG_LAUNCH_CHECK();
-      }
-      ms_settle_k<<<grid_for(n), kBlock, 0, s>>>(n, visited.get(), frontier.get(), next.get(),
-                                                 count.get());
-      UG_LAUNCH_CHECK();
-      UG_CUDA(cudaMemsetAsync(any.get(), 0, 4, s));
-      ms_fold_k<<<1, 64, 0, s>>>(level, k, count.get(), d_reach.get(), d_dsum.get(), d_maxd.get(),
-                                 any.get());
-      UG_LAUNCH_CHECK();
-      if (read_u32(any.get(), s) == 0) break;  // no node reached on this level
-    }
-    UG_CUDA(cudaMemcpyAsync(reach + b0, d_reach.get(), k * 8, cudaMemcpyDeviceToHost, s));
-    UG_CUDA(cudaMemcpyAsync(dsum + b0, d_dsum.get(), k * 8, cudaMemcpyDeviceToHost, s));
-    UG_CUDA(cudaMemcpyAsync(maxd + b0, d_maxd.get(), k * 4, cudaMemcpyDeviceToHost, s));
+  Scratch<unsigned long long> visited(n, s), fa(n, s), fb(n, s), acc(n, s), count(3 * kMsRow, s);
+  Scratch<unsigned long long> d_reach(n_sources, s), d_dsum(n_sources, s);
+  Scratch<uint32_t> d_maxd(n_sources, s), d_src(n_sources, s);
+  Scratch<unsigned> ctl(4, s);
+  UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
+  UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * 8, s));
+  UG_CUDA(cudaMemcpyAsync(d_src.get(), sources, n_sources * 4, cudaMemcpyHostToDevice, s));
+  int per_sm = 0;
+  UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_persist_k, kMsBlock, 0));
+  UG_CHECK(per_sm > 0, URSA_GPU_ECUDA, "msbfs: kernel cannot be resident");
+  const unsigned grid = (unsigned)(per_sm * sm_count(t->device));
+  MsArgs a;
+  a.in_off = t->in.off.get();
+  a.in_src = t->in.tgt.get();
+  a.out_off = t->out.off.get();
+  a.out_tgt = t->out.tgt.get();
+  a.n = n;
+  a.m = t->m;
+  a.sources = d_src.get();
+  a.n_sources = n_sources;
+  a.visited = visited.get();
+  a.fr0 = fa.get();
+  a.fr1 = fb.get();
+  a.acc = acc.get();
+  a.count = count.get();
+  a.reach = d_reach.get();
+  a.dsum = d_dsum.get();
+  a.maxd = d_maxd.get();
+  a.bar = ctl.get();
+  a.err = (int*)(ctl.get() + 2);
+  const uint64_t batches = (n_sources + 63) / 64;
+  for (uint64_t b = 0; b < batches; b += kMsBatchesPerLaunch) {
+    a.b_begin = b;
+    a.b_end = std::min(batches, b + kMsBatchesPerLaunch);
+    void* args[] = {&a};
+    UG_CUDA(cudaLaunchCooperativeKernel((void*)ms_persist_k, dim3(grid), dim3(kMsBlock), args, 0, s));
+    count_launch();
   }
+  int err = 0;
+  UG_CUDA(cudaMemcpyAsync(&err, ctl.get() + 2, 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaMemcpyAsync(reach, d_reach.get(), n_sources * 8, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaMemcpyAsync(dsum, d_dsum.get(), n_sources * 8, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaMemcpyAsync(maxd, d_maxd.get(), n_sources * 4, cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaStreamSynchronize(s));
+  UG_CHECK(err == 0, URSA_GPU_ETIMEOUT, "msbfs: a grid barrier wait expired");
 }
 
 // stats.rs:82-101: `None` -> every node; `Some(frac)` -> k = round(n * frac)
