@@ -44,6 +44,12 @@ nodes, 30% hop(k=2) from a uniform random seed, 20% pagerank (d 0.85, tol
 p50/p99 latency (submit to completion, queueing included).  Beside it the
 plain one-query-per-launch path (shortest_path / k_hop / pagerank C-ABI calls
 from 4 host threads, closed loop) over the same queries.
+
+--workload idmap: Int64 node-id interning of the R-MAT-22 edges, then the
+topology from the dense device columns.
+
+--workload closeness: all-source closeness on R-MAT-16 (65,536 nodes, edge
+factor 16, seed 2); GTEPS = n sources x m edges / time.
 """
 
 from __future__ import annotations
@@ -380,6 +386,147 @@ def run_idmap(args, rank, world):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": k / dt, "unit": "edges/s", "cores": 1, "kind": "port",
                                 "sample": f"serial interning of the first {k:,} edges (the reference interns serially)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+CLOSENESS_SCALE = 16
+CLOSENESS_WORKLOAD = "rmat16_closeness"
+
+
+def closeness_bytes(n: int, m: int, words: int) -> int:
+    """Bytes one 64 x `words`-source batch must move at least once: the
+    in-CSR (4m + 4(n+1)), the out-offsets for the frontier out-edge counts
+    (4(n+1)), and the visited mask array written and read back once
+    (2 x 8 words n)."""
+    return 4 * m + 8 * (n + 1) + 16 * words * n
+
+
+def run_closeness(args, rank, world):
+    """All-source closeness (closeness.rs:69-135) on R-MAT-16 (edge factor 16,
+    seed 2).  value: GTEPS = n sources x m edges / device time of
+    ursa_gpu_closeness_device (events on the launch stream), topology
+    resident, L2 flushed between steps (the graph fits in L2).  e2e: the
+    host C ABI from pinned buffers -- Topology::build + closeness + D2H of
+    the n f64 results.  CPU baseline: the oracle's closeness_one on a strided
+    sample of sources, all host threads."""
+    import torch
+
+    local_rank = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    from ursa_b200 import Topology, _lib, gen
+
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(local_rank))
+    n, src, dst = gen.rmat(CLOSENESS_SCALE, EDGE_FACTOR, SEED)
+    m = int(src.size)
+    topo = Topology.build(n, src, dst)
+    topo.prepare(transpose=True)
+    stream = torch.cuda.Stream()
+    d_out = torch.empty(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
+    ms = C.c_float()
+
+    def dev_step():
+        _lib.check(L.ursa_gpu_closeness_device(topo.handle, d_out.data_ptr(), C.c_void_p(stream.cuda_stream),
+                                               C.byref(ms)))
+        return ms.value
+
+    for _ in range(max(args.warmup, 3)):
+        dev_step()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    launches0 = L.ursa_gpu_launch_count()
+    step_ms, lib_ms = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lib_ms.append(dev_step())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    launches = L.ursa_gpu_launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    t_dev = sum(step_ms) / args.steps
+
+    h_src = torch.from_numpy(src).pin_memory()
+    h_dst = torch.from_numpy(dst).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        h = C.c_void_p()
+        _lib.check(L.ursa_gpu_topo_build(n, h_src.data_ptr(), h_dst.data_ptr(), m, C.byref(h)))
+        try:
+            _lib.check(L.ursa_gpu_closeness(h, h_out.data_ptr()))
+        finally:
+            L.ursa_gpu_topo_free(h)
+
+    e2e_step()
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e.append(time.perf_counter() - t0)
+    t_e2e = sum(e2e) / args.steps
+    words = 4 if n >= 256 and n <= (1 << 21) else 1
+    batches = -(-n // (64 * words))
+    alg = batches * closeness_bytes(n, m, words)
+    peak, peak_kind = load_peaks()
+    achieved = alg / (t_dev * 1e-3) / 1e9
+    line = {
+        "metric": "closeness_gteps",
+        "value": n * m / (t_dev * 1e-3) / 1e9,
+        "unit": "GTEPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_dev,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64 source masks, integer distance folds, f64 quotient",
+        "data": "synthetic",
+        "config": {"workload": CLOSENESS_WORKLOAD, "n_nodes": n, "n_edges": m, "sources": n,
+                   "teps": "n sources x m edges per source", "l2": "flushed between steps (256 MB write)",
+                   "batch_sources": 64 * words},
+        "e2e": {"value": n * m / t_e2e / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 8 * m,
+                "d2h_bytes_per_step": 8 * n, "ms_per_step": 1e3 * t_e2e},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "kernel": "ms_persist_k",
+                     "algorithmic_bytes_per_step": alg,
+                     "note": "one pass over the in-CSR per batch; the graph is L2-resident, so the "
+                             "level count and gather latency bound it, not HBM"},
+        "clocks": clocks,
+        "library_ms": statistics.median(lib_ms),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        O.build()
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        ot = O.Topology(n, src, dst)
+        k = 256
+        while True:
+            srcs = (np.arange(k, dtype=np.uint64) * n // k).astype(np.uint32)
+            t0 = time.perf_counter()
+            O.closeness_sources(ot, srcs)
+            dt = time.perf_counter() - t0
+            if dt >= 3.0 or k >= n:
+                break
+            k = min(n, k * 4)
+        line["cpu_baseline"] = {"value": k * m / dt / 1e9, "unit": "GTEPS", "cores": threads, "kind": "port",
+                                "sample": f"closeness_one from {k:,} strided sources of the same graph"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -777,7 +924,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap"])
+    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap", "closeness"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids (defaults give the benchmark above)
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="pagerank max_iter (rmat22 workload)")
@@ -807,6 +954,9 @@ def main():
         return
     if args.workload == "idmap":
         run_idmap(args, rank, world)
+        return
+    if args.workload == "closeness":
+        run_closeness(args, rank, world)
         return
 
     import torch

@@ -217,9 +217,14 @@ int ursa_gpu_betweenness_weighted(ursa_gpu_topo *t, const double *weights, uint6
 
 /* closeness(&Topology) -> Vec<f64> -- algo/closeness.rs:69-135: per node,
  * reachable / sum of hop distances over the nodes it reaches (out-edges),
- * 0.0 if it reaches none.  A bit-parallel BFS from 64 sources at a time;
- * exact integer folds, so bit-identical to the reference. */
+ * 0.0 if it reaches none.  A bit-parallel BFS from 64 or 256 sources at a
+ * time; exact integer folds, so bit-identical to the reference. */
 int ursa_gpu_closeness(ursa_gpu_topo *t, double *out);
+/* Device-output form of ursa_gpu_closeness: d_out is an n-f64 device array,
+ * enqueued on `stream` (NULL = this thread's stream); returns after the
+ * work completes.  device_ms (may be NULL): device time of the enqueued
+ * work, from events on that stream. */
+int ursa_gpu_closeness_device(ursa_gpu_topo *t, double *d_out, void *stream, float *device_ms);
 /* closeness_weighted(&Topology, &[f64]) -> Vec<f64> -- algo/closeness.rs:
  * 137-224: Dijkstra distances per source (exact), summed in node order. */
 int ursa_gpu_closeness_weighted(ursa_gpu_topo *t, const double *weights, uint64_t n_weights,

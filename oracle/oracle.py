@@ -74,6 +74,7 @@ def lib():
         L.orc_sample_sources.restype = u64
         L.orc_sample_sources.argtypes = [u64, i32, f64, i32, u64, P]
         L.orc_closeness.argtypes = [P, P]
+        L.orc_closeness_sources.argtypes = [P, P, u64, P]
         L.orc_closeness_weighted.argtypes = [P, P, P]
         L.orc_avg_path_length.restype = f64
         L.orc_avg_path_length.argtypes = [P, i32, f64]
@@ -292,6 +293,14 @@ def closeness(t: Topology) -> np.ndarray:
     """closeness (ursa-core/src/algo/closeness.rs:69-135)."""
     out = np.empty(t.n, np.float64)
     lib().orc_closeness(t._h, _p(out))
+    return out
+
+
+def closeness_sources(t: Topology, sources) -> np.ndarray:
+    """closeness_one (closeness.rs:98-128) for the given sources only."""
+    src = np.ascontiguousarray(np.asarray(sources, dtype=np.uint32))
+    out = np.empty(src.size, np.float64)
+    lib().orc_closeness_sources(t._h, _p(src), C.c_uint64(src.size), _p(out))
     return out
 
 

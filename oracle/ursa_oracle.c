@@ -1460,6 +1460,13 @@ void orc_closeness(orc_topo *t, double *out) {
   par_ranges(t->n, par_threads_for(t->n * (t->n + t->m)), clo_range, &c);
 }
 
+/* closeness_one (closeness.rs:98-128) for the given sources only: out[i] is
+ * the closeness of sources[i]. */
+void orc_closeness_sources(orc_topo *t, const uint32_t *sources, uint64_t k, double *out) {
+  clo_ctx c = {t, NULL, sources, out, NULL, NULL, NULL};
+  par_ranges(k, par_threads_for(k * (t->n + t->m)), clo_range, &c);
+}
+
 static void clow_range(void *p, uint64_t lo, uint64_t hi, int tid) {
   (void)tid;
   clo_ctx *c = (clo_ctx *)p;

@@ -33,6 +33,7 @@ uint64_t orc_idmap_build(const int64_t *src, const int64_t *dst, uint64_t n_edge
 /* closeness / closeness_weighted (algo/closeness.rs:69-224) and
  * avg_path_length / diameter (ursa-plan/src/stats.rs:82-167). */
 void orc_closeness(orc_topo *t, double *out);
+void orc_closeness_sources(orc_topo *t, const uint32_t *sources, uint64_t k, double *out);
 void orc_closeness_weighted(orc_topo *t, const double *weights, double *out);
 double orc_avg_path_length(orc_topo *t, int has_sample, double sample);
 int64_t orc_diameter(orc_topo *t, int approximate);

@@ -79,3 +79,20 @@ def test_reference_goldens():
     assert algo.avg_path_length(tri) == 1.5 and algo.diameter(tri, False) == 2  # stats.rs
     two = Topology.build(4, [0, 2], [1, 3])
     assert algo.avg_path_length(two) == 1.0 and algo.diameter(two, False) == 1
+
+
+def test_closeness_device_output(orc):
+    """ursa_gpu_closeness_device: same bits as the host form, device time > 0."""
+    import ctypes as C
+
+    import torch
+
+    from ursa_b200 import Topology, _lib, algo, gen
+
+    n, s, d = gen.rmat(12, 8, 3)
+    g = Topology.build(n, s, d)
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    ms = C.c_float()
+    _lib.check(_lib.load().ursa_gpu_closeness_device(g.handle, out.data_ptr(), None, C.byref(ms)))
+    assert np.array_equal(_bits(out.cpu().numpy()), _bits(algo.closeness(g)))
+    assert ms.value > 0.0

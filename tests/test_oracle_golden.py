@@ -454,3 +454,13 @@ def test_path_stats_goldens(orc):
     assert orc.diameter(T(4, [0, 1, 2], [1, 2, 3]), False) == 3
     two = T(4, [0, 2], [1, 3])
     assert abs(orc.avg_path_length(two) - 1.0) < 1e-12 and orc.diameter(two, False) == 1
+
+
+def test_closeness_sources_matches_full(orc):
+    from cases import random_graph
+
+    n, s, d = random_graph(500, 2000, 11)
+    t = orc.Topology(n, s, d)
+    full = orc.closeness(t)
+    src = np.array([0, 7, 499, 250, 7], np.uint32)
+    assert np.array_equal(orc.closeness_sources(t, src), full[src])

@@ -170,6 +170,7 @@ SIGNATURES = {
     "ursa_gpu_batch_results": (i32, [P, P, P, P, P, P]),
     "ursa_gpu_batch_device_results": (i32, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "ursa_gpu_closeness": (i32, [P, P]),
+    "ursa_gpu_closeness_device": (i32, [P, P, P, C.POINTER(C.c_float)]),
     "ursa_gpu_closeness_weighted": (i32, [P, P, u64, P]),
     "ursa_gpu_avg_path_length": (i32, [P, i32, f64, C.POINTER(f64)]),
     "ursa_gpu_diameter": (i32, [P, i32, C.POINTER(i64)]),

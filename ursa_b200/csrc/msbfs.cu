@@ -41,10 +41,89 @@ namespace {
 
 constexpr int kMsBlock = 256;
 constexpr int kMsWarps = kMsBlock / 32;
-constexpr uint64_t kMsBatchesPerLaunch = 16;
+constexpr uint64_t kMsSourcesPerLaunch = 1024;
 constexpr uint64_t kMsWaitNs = 5000000000ull;  // one grid-barrier wait
-constexpr int kMsRow = 72;  // per-level counter row: 64 per-source counts, [64] = frontier out-edges
 constexpr uint64_t kMsPushDiv = 8;  // push while the frontier's out-edges are below m / 8
+
+// W 64-bit words per node: bit j of word q belongs to source 64 q + j of the
+// batch.  A node's W words are contiguous (one 32-byte sector for W = 4).
+template <int W>
+struct Msk {
+  unsigned long long v[W];
+};
+
+template <int W>
+__device__ __forceinline__ Msk<W> mk_zero() {
+  Msk<W> r;
+#pragma unroll
+  for (int q = 0; q < W; q++) r.v[q] = 0;
+  return r;
+}
+template <int W>
+__device__ __forceinline__ Msk<W> mk_load(const unsigned long long* p, uint64_t node) {
+  Msk<W> r;
+  p += node * W;
+  if constexpr (W == 1) {
+    r.v[0] = __ldcg(p);
+  } else {
+#pragma unroll
+    for (int q = 0; q < W; q += 2) {
+      const ulonglong2 x = __ldcg(reinterpret_cast<const ulonglong2*>(p + q));
+      r.v[q] = x.x;
+      r.v[q + 1] = x.y;
+    }
+  }
+  return r;
+}
+template <int W>
+__device__ __forceinline__ void mk_store(unsigned long long* p, uint64_t node, const Msk<W>& m) {
+  p += node * W;
+  if constexpr (W == 1) {
+    p[0] = m.v[0];
+  } else {
+#pragma unroll
+    for (int q = 0; q < W; q += 2)
+      *reinterpret_cast<ulonglong2*>(p + q) = make_ulonglong2(m.v[q], m.v[q + 1]);
+  }
+}
+template <int W>
+__device__ __forceinline__ bool mk_any(const Msk<W>& m) {
+  unsigned long long x = 0;
+#pragma unroll
+  for (int q = 0; q < W; q++) x |= m.v[q];
+  return x != 0;
+}
+template <int W>
+__device__ __forceinline__ Msk<W> mk_andnot(const Msk<W>& a, const Msk<W>& b) {  // a & ~b
+  Msk<W> r;
+#pragma unroll
+  for (int q = 0; q < W; q++) r.v[q] = a.v[q] & ~b.v[q];
+  return r;
+}
+template <int W>
+__device__ __forceinline__ void mk_or(Msk<W>& a, const Msk<W>& b) {
+#pragma unroll
+  for (int q = 0; q < W; q++) a.v[q] |= b.v[q];
+}
+template <int W>
+__device__ __forceinline__ bool mk_covers(const Msk<W>& acc, const Msk<W>& need) {  // need ⊆ acc
+  unsigned long long x = 0;
+#pragma unroll
+  for (int q = 0; q < W; q++) x |= need.v[q] & ~acc.v[q];
+  return x == 0;
+}
+template <int W>
+__device__ __forceinline__ Msk<W> mk_shfl(const Msk<W>& m, int j) {
+  Msk<W> r;
+#pragma unroll
+  for (int q = 0; q < W; q++) r.v[q] = __shfl_sync(0xffffffffu, m.v[q], j);
+  return r;
+}
+__device__ __forceinline__ unsigned long long warp_or64(unsigned long long v) {
+  const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)v);
+  const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(v >> 32));
+  return ((unsigned long long)hi << 32) | lo;
+}
 
 struct MsArgs {
   const uint32_t* in_off;
@@ -54,12 +133,12 @@ struct MsArgs {
   uint64_t n, m;
   const uint32_t* sources;  // n_sources ids < n
   uint64_t n_sources;
-  uint64_t b_begin, b_end;  // batches of 64 sources run by this launch
-  unsigned long long* visited;
-  unsigned long long* fr0;    // frontier masks, odd levels' input
-  unsigned long long* fr1;    // even levels' input
-  unsigned long long* acc;    // pushed masks of a top-down level; all zero between levels
-  unsigned long long* count;  // 3 rows of kMsRow, row = level % 3
+  uint64_t b_begin, b_end;  // batches of 64 W sources run by this launch
+  unsigned long long* visited;  // n W words each
+  unsigned long long* fr0;      // frontier masks, odd levels' input
+  unsigned long long* fr1;      // even levels' input
+  unsigned long long* acc;      // pushed masks of a top-down level; all zero between levels
+  unsigned long long* count;    // 3 rows of 64 W + 8, row = level % 3; [64 W] = frontier out-edges
   unsigned long long* reach;
   unsigned long long* dsum;
   uint32_t* maxd;
@@ -67,33 +146,30 @@ struct MsArgs {
   int* err;
 };
 
-__device__ __forceinline__ unsigned long long warp_or64(unsigned long long v) {
-  const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)v);
-  const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(v >> 32));
-  return ((unsigned long long)hi << 32) | lo;
-}
-
 // Top-down half of a level: every frontier node v ORs its mask into acc[w]
 // for each out-edge v -> w whose target still lacks some of those sources.
+template <int W>
 __device__ __forceinline__ void ms_push(const MsArgs& a, const unsigned long long* cur, uint64_t gwarp,
                                         uint64_t nwarps, int lane) {
   for (uint64_t c0 = gwarp * 32; c0 < a.n; c0 += nwarps * 32) {
     const uint64_t v = c0 + lane;
-    unsigned long long f = 0;
+    Msk<W> f = mk_zero<W>();
     uint32_t e0 = 0, e1 = 0;
     if (v < a.n) {
-      f = __ldcg(&cur[v]);
-      if (f) {
+      f = mk_load<W>(cur, v);
+      if (mk_any(f)) {
         e0 = __ldg(&a.out_off[v]);
         e1 = __ldg(&a.out_off[v + 1]);
       }
     }
-    const bool heavy = f && e1 - e0 > 32;
-    if (f && !heavy) {
+    const bool heavy = e1 - e0 > 32;
+    if (!heavy) {
       for (uint32_t e = e0; e < e1; e++) {
         const uint32_t w = __ldg(&a.out_tgt[e]);
-        const unsigned long long add = f & ~__ldcg(&a.visited[w]);
-        if (add) atomicOr(&a.acc[w], add);
+        const Msk<W> add = mk_andnot(f, mk_load<W>(a.visited, w));
+#pragma unroll
+        for (int q = 0; q < W; q++)
+          if (add.v[q]) atomicOr(&a.acc[(uint64_t)w * W + q], add.v[q]);
       }
     }
     unsigned hm = __ballot_sync(0xffffffffu, heavy);
@@ -101,20 +177,26 @@ __device__ __forceinline__ void ms_push(const MsArgs& a, const unsigned long lon
       const int j = __ffs(hm) - 1;
       hm &= hm - 1;
       const uint32_t h0 = __shfl_sync(0xffffffffu, e0, j), h1 = __shfl_sync(0xffffffffu, e1, j);
-      const unsigned long long hf = __shfl_sync(0xffffffffu, f, j);
+      const Msk<W> hf = mk_shfl(f, j);
       for (uint32_t e = h0 + lane; e < h1; e += 32) {
         const uint32_t w = __ldg(&a.out_tgt[e]);
-        const unsigned long long add = hf & ~__ldcg(&a.visited[w]);
-        if (add) atomicOr(&a.acc[w], add);
+        const Msk<W> add = mk_andnot(hf, mk_load<W>(a.visited, w));
+#pragma unroll
+        for (int q = 0; q < W; q++)
+          if (add.v[q]) atomicOr(&a.acc[(uint64_t)w * W + q], add.v[q]);
       }
     }
   }
 }
 
+template <int W>
 __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
-  __shared__ unsigned sc[64];
+  constexpr int S = 64 * W;     // sources per batch
+  constexpr int R = 64 * W + 8;  // counter row length
+  static_assert(S <= kMsBlock, "one thread per source of a batch");
+  __shared__ unsigned sc[S];
   __shared__ unsigned long long s_mf;
-  __shared__ unsigned s_act[2];
+  __shared__ unsigned s_act[2 * W];
   const int lane = threadIdx.x & 31;
   const uint64_t n = a.n;
   const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
@@ -122,82 +204,89 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (uint64_t bt = a.b_begin; bt < a.b_end; bt++) {
-    const uint64_t s0 = bt * 64;
+    const uint64_t s0 = bt * S;
     const uint64_t left = a.n_sources - s0;
-    const uint32_t k = left < 64 ? (uint32_t)left : 64u;
-    const unsigned long long full = k == 64 ? ~0ull : ((1ull << k) - 1);
-    for (uint64_t w = gtid; w < n; w += nthreads) {
-      a.visited[w] = 0;
-      a.fr0[w] = 0;
+    const uint32_t k = left < (uint64_t)S ? (uint32_t)left : (uint32_t)S;
+    Msk<W> active;  // sources whose search still grows
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      const int bits = (int)k - 64 * q;
+      active.v[q] = bits >= 64 ? ~0ull : (bits <= 0 ? 0ull : ((1ull << bits) - 1));
+    }
+    for (uint64_t x = gtid; x < n * W; x += nthreads) {
+      a.visited[x] = 0;
+      a.fr0[x] = 0;
     }
     grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
     if (*(volatile int*)a.err) return;
     if (blockIdx.x == 0) {  // every block has read the previous batch's last counter row
-      if (threadIdx.x < 3 * kMsRow) a.count[threadIdx.x] = 0;
+      for (int x = threadIdx.x; x < 3 * R; x += kMsBlock) a.count[x] = 0;
       __syncthreads();
       if (threadIdx.x < k) {
         const uint32_t src = a.sources[s0 + threadIdx.x];
-        atomicOr(&a.visited[src], 1ull << threadIdx.x);
-        atomicOr(&a.fr0[src], 1ull << threadIdx.x);
-        atomicAdd(&a.count[64], (unsigned long long)(a.out_off[src + 1] - a.out_off[src]));
+        const uint64_t wd = (uint64_t)src * W + (threadIdx.x >> 6);
+        atomicOr(&a.visited[wd], 1ull << (threadIdx.x & 63));
+        atomicOr(&a.fr0[wd], 1ull << (threadIdx.x & 63));
+        atomicAdd(&a.count[S], (unsigned long long)(a.out_off[src + 1] - a.out_off[src]));
       }
     }
     grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
     if (*(volatile int*)a.err) return;
     unsigned long long reach = 0, dsum = 0;  // block 0, thread b < k: source s0 + b
     uint32_t maxd = 0;
-    unsigned long long active = full;  // sources whose search still grows
     for (uint32_t level = 1;; level++) {
       const unsigned long long* cur = (level & 1) ? a.fr0 : a.fr1;
       unsigned long long* nxt = (level & 1) ? a.fr1 : a.fr0;
-      unsigned long long* row = a.count + (level % 3) * kMsRow;
-      const unsigned long long mf = __ldcg(&a.count[((level - 1) % 3) * kMsRow + 64]);
+      unsigned long long* row = a.count + (level % 3) * R;
+      const unsigned long long mf = __ldcg(&a.count[((level - 1) % 3) * R + S]);
       const bool push = mf * kMsPushDiv < a.m;
-      if (threadIdx.x < 64) sc[threadIdx.x] = 0;
+      for (int x = threadIdx.x; x < S; x += kMsBlock) sc[x] = 0;
       if (threadIdx.x == 0) s_mf = 0;
       // row (level + 1) % 3 was last read before the previous barrier
-      if (blockIdx.x == 0 && threadIdx.x < kMsRow) a.count[((level + 1) % 3) * kMsRow + threadIdx.x] = 0;
+      if (blockIdx.x == 0)
+        for (int x = threadIdx.x; x < R; x += kMsBlock) a.count[((level + 1) % 3) * R + x] = 0;
       __syncthreads();
       if (push) {
-        ms_push(a, cur, gwarp, nwarps, lane);
+        ms_push<W>(a, cur, gwarp, nwarps, lane);
         grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
         if (*(volatile int*)a.err) return;
       }
       for (uint64_t c0 = gwarp * 32; c0 < n; c0 += nwarps * 32) {
         const uint64_t w = c0 + lane;
-        unsigned long long vis = 0, nw = 0;
+        Msk<W> vis = mk_zero<W>(), nw = mk_zero<W>();
         if (push) {
           if (w < n) {
-            const unsigned long long p = __ldcg(&a.acc[w]);
-            if (p) {
-              a.acc[w] = 0;
-              vis = __ldcg(&a.visited[w]);
-              nw = p & ~vis;
+            const Msk<W> p = mk_load<W>(a.acc, w);
+            if (mk_any(p)) {
+              mk_store<W>(a.acc, w, mk_zero<W>());
+              vis = mk_load<W>(a.visited, w);
+              nw = mk_andnot(p, vis);
             }
           }
         } else {
           // bottom-up: OR the in-neighbours' frontier masks until every
           // needed source is found
-          unsigned long long need = 0, acc = 0;
+          Msk<W> need = mk_zero<W>(), acc = mk_zero<W>();
           uint32_t e0 = 0, e1 = 0;
           if (w < n) {
-            vis = __ldcg(&a.visited[w]);
-            need = active & ~vis;
-            if (need) {
+            vis = mk_load<W>(a.visited, w);
+            need = mk_andnot(active, vis);
+            if (mk_any(need)) {
               e0 = __ldg(&a.in_off[w]);
               e1 = __ldg(&a.in_off[w + 1]);
             }
           }
-          const bool heavy = need && e1 - e0 > 32;
-          if (need && !heavy) {
-            for (uint32_t e = e0; e < e1; e += 4) {
-              const uint32_t r = e1 - e;
-              const uint32_t v0 = __ldg(&a.in_src[e]);
-              const uint32_t v1 = r > 1 ? __ldg(&a.in_src[e + 1]) : v0;
-              const uint32_t v2 = r > 2 ? __ldg(&a.in_src[e + 2]) : v0;
-              const uint32_t v3 = r > 3 ? __ldg(&a.in_src[e + 3]) : v0;
-              acc |= __ldcg(&cur[v0]) | __ldcg(&cur[v1]) | __ldcg(&cur[v2]) | __ldcg(&cur[v3]);
-              if ((acc & need) == need) break;
+          const bool heavy = e1 - e0 > 32;
+          if (!heavy) {
+            constexpr int UL = W == 1 ? 4 : 2;  // in-edges per step
+            for (uint32_t e = e0; e < e1; e += UL) {
+              uint32_t v[UL];
+              v[0] = __ldg(&a.in_src[e]);
+#pragma unroll
+              for (int q = 1; q < UL; q++) v[q] = e + q < e1 ? __ldg(&a.in_src[e + q]) : v[0];
+#pragma unroll
+              for (int q = 0; q < UL; q++) mk_or(acc, mk_load<W>(cur, v[q]));
+              if (mk_covers(acc, need)) break;
             }
           }
           unsigned hm = __ballot_sync(0xffffffffu, heavy);
@@ -205,60 +294,71 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
             const int j = __ffs(hm) - 1;
             hm &= hm - 1;
             const uint32_t h0 = __shfl_sync(0xffffffffu, e0, j), h1 = __shfl_sync(0xffffffffu, e1, j);
-            const unsigned long long hneed = __shfl_sync(0xffffffffu, need, j);
-            unsigned long long hacc = 0;
-            for (uint32_t e = h0; e < h1; e += 128) {
-              unsigned long long f = 0;
+            const Msk<W> hneed = mk_shfl(need, j);
+            Msk<W> hacc = mk_zero<W>();
+            constexpr int U = W == 1 ? 4 : 2;  // in-edges per lane per step
+            for (uint32_t e = h0; e < h1; e += 32 * U) {
+              Msk<W> f = mk_zero<W>();
 #pragma unroll
-              for (int q = 0; q < 4; q++) {
+              for (int q = 0; q < U; q++) {
                 const uint32_t x = e + q * 32 + lane;
-                if (x < h1) f |= __ldcg(&cur[__ldg(&a.in_src[x])]);
+                if (x < h1) mk_or(f, mk_load<W>(cur, __ldg(&a.in_src[x])));
               }
-              hacc |= warp_or64(f);
-              if ((hacc & hneed) == hneed) break;
+#pragma unroll
+              for (int q = 0; q < W; q++) hacc.v[q] |= warp_or64(f.v[q]);
+              if (mk_covers(hacc, hneed)) break;
             }
             if (lane == j) acc = hacc;
           }
-          nw = acc & need;
+#pragma unroll
+          for (int q = 0; q < W; q++) nw.v[q] = acc.v[q] & need.v[q];
         }
         unsigned long long od = 0;
+        const bool got = mk_any(nw);
         if (w < n) {
-          if (nw) {
-            a.visited[w] = vis | nw;
+          if (got) {
+            Msk<W> nv = vis;
+            mk_or(nv, nw);
+            mk_store<W>(a.visited, w, nv);
             od = __ldg(&a.out_off[w + 1]) - __ldg(&a.out_off[w]);
           }
-          nxt[w] = nw;
+          mk_store<W>(nxt, w, nw);
         }
-        if (__any_sync(0xffffffffu, nw != 0)) {
+        if (__any_sync(0xffffffffu, got)) {
+#pragma unroll
+          for (int q = 0; q < W; q++) {
+            if (!__any_sync(0xffffffffu, nw.v[q] != 0)) continue;
 #pragma unroll 8
-          for (int b = 0; b < 64; b++) {
-            const unsigned c = __popc(__ballot_sync(0xffffffffu, (nw >> b) & 1ull));
-            if (lane == 0 && c) atomicAdd(&sc[b], c);
+            for (int b = 0; b < 64; b++) {
+              const unsigned c = __popc(__ballot_sync(0xffffffffu, (nw.v[q] >> b) & 1ull));
+              if (lane == 0 && c) atomicAdd(&sc[64 * q + b], c);
+            }
           }
           for (int o = 16; o; o >>= 1) od += __shfl_down_sync(0xffffffffu, od, o);
           if (lane == 0) atomicAdd(&s_mf, od);
         }
       }
       __syncthreads();
-      if (threadIdx.x < 64 && sc[threadIdx.x])
-        atomicAdd(&row[threadIdx.x], (unsigned long long)sc[threadIdx.x]);
-      if (threadIdx.x == 0 && s_mf) atomicAdd(&row[64], s_mf);
+      for (int x = threadIdx.x; x < S; x += kMsBlock)
+        if (sc[x]) atomicAdd(&row[x], (unsigned long long)sc[x]);
+      if (threadIdx.x == 0 && s_mf) atomicAdd(&row[S], s_mf);
       grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
       if (*(volatile int*)a.err) return;
       unsigned long long c = 0;
-      if (threadIdx.x < 64) c = __ldcg(&row[threadIdx.x]);
+      if (threadIdx.x < S) c = __ldcg(&row[threadIdx.x]);
       if (blockIdx.x == 0 && c) {  // only bits < k are ever counted
         reach += c;
         dsum += (unsigned long long)level * c;
         maxd = level;
       }
       const unsigned bal = __ballot_sync(0xffffffffu, c != 0);
-      if (threadIdx.x == 0) s_act[0] = bal;
-      if (threadIdx.x == 32) s_act[1] = bal;
+      if (lane == 0 && threadIdx.x < S) s_act[threadIdx.x >> 5] = bal;
       __syncthreads();
       // a source that reached nobody new on this level is finished
-      active = ((unsigned long long)s_act[1] << 32) | s_act[0];
-      if (!active) break;
+#pragma unroll
+      for (int q = 0; q < W; q++)
+        active.v[q] = ((unsigned long long)s_act[2 * q + 1] << 32) | s_act[2 * q];
+      if (!mk_any(active)) break;
     }
     if (blockIdx.x == 0 && threadIdx.x < k) {
       a.reach[s0 + threadIdx.x] = reach;
@@ -268,27 +368,63 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
   }
 }
 
+template <int W>
+void ms_launch(MsArgs a, uint64_t n_sources, int device, cudaStream_t s) {
+  int per_sm = 0;
+  UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_persist_k<W>, kMsBlock, 0));
+  UG_CHECK(per_sm > 0, URSA_GPU_ECUDA, "msbfs: kernel cannot be resident");
+  // one warp per 32 nodes is all a level pass uses; fewer blocks make
+  // cheaper grid barriers
+  const uint64_t want = (a.n + 32 * kMsWarps - 1) / (32 * kMsWarps);
+  const uint64_t cap = (uint64_t)per_sm * sm_count(device);
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
+  const uint64_t batches = (n_sources + 64 * W - 1) / (64 * W);
+  const uint64_t per_launch = std::max<uint64_t>(1, kMsSourcesPerLaunch / (64 * W));
+  for (uint64_t b = 0; b < batches; b += per_launch) {
+    a.b_begin = b;
+    a.b_end = std::min(batches, b + per_launch);
+    void* args[] = {&a};
+    UG_CUDA(cudaLaunchCooperativeKernel((void*)ms_persist_k<W>, dim3(grid), dim3(kMsBlock), args, 0, s));
+    count_launch();
+  }
+}
+
+
+__global__ void ms_iota_k(uint32_t* out, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)i;
+}
+
+// closeness.rs:117-127: reachable as f64 / sum as f64, 0.0 if the sum is 0
+// (IEEE division, correctly rounded as on the host).
+__global__ void ms_closeness_k(const unsigned long long* __restrict__ reach,
+                               const unsigned long long* __restrict__ dsum, uint64_t n, double* out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = dsum[i] > 0 ? (double)(long long)reach[i] / (double)(long long)dsum[i] : 0.0;
+}
+
 }  // namespace
 
-// Per-source BFS folds (reach = nodes at distance >= 1, dsum = their summed
-// distances, maxd = eccentricity) for `sources` (host ids < n), following
-// out-edges.  Outputs are host arrays of n_sources entries.
-void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_t* reach,
-               uint64_t* dsum, uint32_t* maxd, cudaStream_t s) {
+// Enqueues the per-source BFS folds (reach = nodes at distance >= 1, dsum =
+// their summed distances, maxd = eccentricity) for the device ids d_src
+// (< n), following out-edges, into device arrays of n_sources entries.
+// d_ctl: 4 zeroed words (grid barrier; word 2 turns nonzero if a barrier
+// wait expired).  Batches are 256 sources wide when there are enough
+// sources to fill them and the masks of a graph of at most 2^21 nodes (64 MB
+// per mask array) stay in L2; otherwise 64 wide (fewer registers per
+// thread, more warps per SM).
+static void msbfs_enqueue(TopoImpl* t, const uint32_t* d_src, uint64_t n_sources,
+                          unsigned long long* d_reach, unsigned long long* d_dsum, uint32_t* d_maxd,
+                          unsigned* d_ctl, cudaStream_t s) {
   const uint64_t n = t->n;
   if (n_sources == 0) return;
   ensure_in(t, s);
-  Scratch<unsigned long long> visited(n, s), fa(n, s), fb(n, s), acc(n, s), count(3 * kMsRow, s);
-  Scratch<unsigned long long> d_reach(n_sources, s), d_dsum(n_sources, s);
-  Scratch<uint32_t> d_maxd(n_sources, s), d_src(n_sources, s);
-  Scratch<unsigned> ctl(4, s);
-  UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
-  UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * 8, s));
-  UG_CUDA(cudaMemcpyAsync(d_src.get(), sources, n_sources * 4, cudaMemcpyHostToDevice, s));
-  int per_sm = 0;
-  UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_persist_k, kMsBlock, 0));
-  UG_CHECK(per_sm > 0, URSA_GPU_ECUDA, "msbfs: kernel cannot be resident");
-  const unsigned grid = (unsigned)(per_sm * sm_count(t->device));
+  const int W = n_sources >= 256 && n <= (1ull << 21) ? 4 : 1;
+  Scratch<unsigned long long> visited(n * W, s), fa(n * W, s), fb(n * W, s), acc(n * W, s);
+  Scratch<unsigned long long> count(3 * (64 * W + 8), s);
+  UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * W * 8, s));
   MsArgs a;
   a.in_off = t->in.off.get();
   a.in_src = t->in.tgt.get();
@@ -296,26 +432,34 @@ void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_
   a.out_tgt = t->out.tgt.get();
   a.n = n;
   a.m = t->m;
-  a.sources = d_src.get();
+  a.sources = d_src;
   a.n_sources = n_sources;
   a.visited = visited.get();
   a.fr0 = fa.get();
   a.fr1 = fb.get();
   a.acc = acc.get();
   a.count = count.get();
-  a.reach = d_reach.get();
-  a.dsum = d_dsum.get();
-  a.maxd = d_maxd.get();
-  a.bar = ctl.get();
-  a.err = (int*)(ctl.get() + 2);
-  const uint64_t batches = (n_sources + 63) / 64;
-  for (uint64_t b = 0; b < batches; b += kMsBatchesPerLaunch) {
-    a.b_begin = b;
-    a.b_end = std::min(batches, b + kMsBatchesPerLaunch);
-    void* args[] = {&a};
-    UG_CUDA(cudaLaunchCooperativeKernel((void*)ms_persist_k, dim3(grid), dim3(kMsBlock), args, 0, s));
-    count_launch();
-  }
+  a.reach = d_reach;
+  a.dsum = d_dsum;
+  a.maxd = d_maxd;
+  a.bar = d_ctl;
+  a.err = (int*)(d_ctl + 2);
+  if (W == 4)
+    ms_launch<4>(a, n_sources, t->device, s);
+  else
+    ms_launch<1>(a, n_sources, t->device, s);
+}
+
+// Host form of msbfs_enqueue: host sources in, host folds out.
+void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_t* reach,
+               uint64_t* dsum, uint32_t* maxd, cudaStream_t s) {
+  if (n_sources == 0) return;
+  Scratch<unsigned long long> d_reach(n_sources, s), d_dsum(n_sources, s);
+  Scratch<uint32_t> d_maxd(n_sources, s), d_src(n_sources, s);
+  Scratch<unsigned> ctl(4, s);
+  UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
+  UG_CUDA(cudaMemcpyAsync(d_src.get(), sources, n_sources * 4, cudaMemcpyHostToDevice, s));
+  msbfs_enqueue(t, d_src.get(), n_sources, d_reach.get(), d_dsum.get(), d_maxd.get(), ctl.get(), s);
   int err = 0;
   UG_CUDA(cudaMemcpyAsync(&err, ctl.get() + 2, 4, cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaMemcpyAsync(reach, d_reach.get(), n_sources * 8, cudaMemcpyDeviceToHost, s));
@@ -323,6 +467,35 @@ void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_
   UG_CUDA(cudaMemcpyAsync(maxd, d_maxd.get(), n_sources * 4, cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaStreamSynchronize(s));
   UG_CHECK(err == 0, URSA_GPU_ETIMEOUT, "msbfs: a grid barrier wait expired");
+}
+
+// Closeness of every node into the device array d_out, enqueued on s;
+// returns after completion, with the device time of the enqueued work.
+static void closeness_device(TopoImpl* t, double* d_out, cudaStream_t s, float* device_ms) {
+  const uint64_t n = t->n;
+  Scratch<unsigned long long> d_reach(n, s), d_dsum(n, s);
+  Scratch<uint32_t> d_maxd(n, s), d_src(n, s);
+  Scratch<unsigned> ctl(4, s);
+  cudaEvent_t e0, e1;
+  UG_CUDA(cudaEventCreate(&e0));
+  UG_CUDA(cudaEventCreate(&e1));
+  UG_CUDA(cudaEventRecord(e0, s));
+  UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
+  ms_iota_k<<<grid_for(n), kBlock, 0, s>>>(d_src.get(), n);
+  UG_LAUNCH_CHECK();
+  msbfs_enqueue(t, d_src.get(), n, d_reach.get(), d_dsum.get(), d_maxd.get(), ctl.get(), s);
+  ms_closeness_k<<<grid_for(n), kBlock, 0, s>>>(d_reach.get(), d_dsum.get(), n, d_out);
+  UG_LAUNCH_CHECK();
+  UG_CUDA(cudaEventRecord(e1, s));
+  int err = 0;
+  UG_CUDA(cudaMemcpyAsync(&err, ctl.get() + 2, 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (device_ms) *device_ms = ms;
+  UG_CHECK(err == 0, URSA_GPU_ETIMEOUT, "closeness: a grid barrier wait expired");
 }
 
 // stats.rs:82-101: `None` -> every node; `Some(frac)` -> k = round(n * frac)
@@ -364,14 +537,23 @@ int ursa_gpu_closeness(ursa_gpu_topo* t, double* out) {
     if (n == 0) return;
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);
-    std::vector<uint32_t> src(n);
-    for (uint64_t i = 0; i < n; i++) src[i] = (uint32_t)i;
-    std::vector<uint64_t> reach(n), dsum(n);
-    std::vector<uint32_t> maxd(n);
-    msbfs_run(ti, src.data(), n, reach.data(), dsum.data(), maxd.data(), s);
-    // closeness.rs:117-127: reachable as f64 / sum as f64, 0.0 if sum == 0
-    for (uint64_t u = 0; u < n; u++)
-      out[u] = dsum[u] > 0 ? (double)(int64_t)reach[u] / (double)(int64_t)dsum[u] : 0.0;
+    Scratch<double> d_out(n, s);
+    closeness_device(ti, d_out.get(), s, nullptr);
+    UG_CUDA(cudaMemcpyAsync(out, d_out.get(), n * 8, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int ursa_gpu_closeness_device(ursa_gpu_topo* t, double* d_out, void* stream, float* device_ms) {
+  return guard([&] {
+    UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
+    TopoImpl* ti = &t->impl;
+    if (device_ms) *device_ms = 0.f;
+    if (ti->n == 0) return;
+    UG_CHECK(d_out, URSA_GPU_EINVAL, "d_out is NULL");
+    cudaStream_t ts = thread_stream(ti->device);  // also selects the device
+    cudaStream_t s = stream ? (cudaStream_t)stream : ts;
+    closeness_device(ti, d_out, s, device_ms);
   });
 }
 
