@@ -388,6 +388,7 @@ int ursa_gpu_betweenness_weighted(ursa_gpu_topo* t, const double* weights, uint6
     UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
+    check_sssp_weights(weights, ti->m);
     if (ti->n == 0) return;  // betweenness.rs:248-250
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);

@@ -46,6 +46,17 @@ void count_launch();
 
 constexpr int kBlock = 256;
 
+// Edge weights for the shortest-path family: non-null when there are edges
+// and none negative, as evaluate_weight requires before any weighted kernel
+// runs (ursa-plan/src/weight.rs:88-93).  Negative weights would also let a
+// frontier Bellman-Ford cycle forever.
+inline void check_sssp_weights(const double* w, uint64_t m) {
+  if (m == 0) return;
+  if (!w) throw Error(URSA_GPU_EINVAL, "weights is NULL");
+  for (uint64_t i = 0; i < m; i++)
+    if (w[i] < 0.0) throw Error(URSA_GPU_EINVAL, "weights must be non-negative");
+}
+
 inline unsigned grid_for(uint64_t n, int block = kBlock, unsigned cap = 148u * 32u) {
   uint64_t g = (n + block - 1) / block;
   if (g < 1) g = 1;

@@ -34,9 +34,6 @@
 
 namespace ug {
 
-void dijkstra_run(TopoImpl* t, const double* d_weights, uint32_t source, int dir, double* d_out,
-                  cudaStream_t s);
-
 namespace {
 
 constexpr int kMsBlock = 256;
@@ -390,6 +387,162 @@ void ms_launch(MsArgs a, uint64_t n_sources, int device, cudaStream_t s) {
 }
 
 
+// ---- weighted closeness (closeness.rs:137-224), many sources at once ----
+//
+// A batch is G sub-rows of 32 sources; lane l of a warp works for source
+// 32 sub + l.  dist is node-major (n x 32 G distance bit patterns) and
+// flags[v G + sub] marks the sources whose distance at v fell in the last
+// round.  A round (ending in a grid barrier) walks the out-CSR in 32-edge
+// chunks, one (chunk, sub-row) per warp, so a hub's edges spread over many
+// warps: for each edge v -> w of weight x whose source v is flagged, the
+// flagged lanes relax dist[w] = min(dist[w], fl(dist[v] + x)) with an
+// atomicMin on the bits (non-negative doubles order like their bit
+// patterns) and flag w for the next round where they lowered it.  Three
+// flag buffers rotate: a round reads one, sets the next and clears the one
+// read two rounds before.  Rounds end when one lowers nothing.
+// The fixpoint is Dijkstra's: dist[v] = min over in-edges of fl(dist[u] + x),
+// the minimum left-to-right f64 path sum (fl(a + x) is monotone in a and
+// >= a for x >= 0).  Each lane then folds its source's distances in node
+// order exactly as closeness_weighted does (f64 sum over reachable v != u).
+
+constexpr unsigned long long kWsInf = 0x7FF0000000000000ull;
+constexpr uint64_t kWsDistBudget = 64ull << 20;  // distance rows of one batch: stay in L2
+
+struct WsArgs {
+  const uint32_t* off;   // out-CSR
+  const uint32_t* tgt;
+  const uint32_t* esrc;  // source node of each out-CSR slot
+  const double* wt;      // weights in out-CSR slot order
+  uint64_t n, m;
+  const uint32_t* sources;  // n_sources ids < n
+  uint64_t n_sources;
+  uint64_t b_begin, b_end;  // batches of 32 G sources run by this launch
+  unsigned G;
+  unsigned long long* dist;  // n x 32 G
+  uint32_t* fl[3];           // n x G flags each; round r reads fl[r % 3]
+  unsigned long long* count;  // 3 counters, index round % 3: blocks that lowered a distance
+  double* out;               // closeness per source
+  unsigned* bar;
+  int* err;
+};
+
+__global__ void __launch_bounds__(kMsBlock) ws_persist_k(WsArgs a) {
+  __shared__ int s_any;
+  const int lane = threadIdx.x & 31;
+  const uint64_t n = a.n, m = a.m, G = a.G, S = 32ull * a.G;
+  const uint64_t nwarps = (uint64_t)gridDim.x * kMsWarps;
+  const uint64_t gwarp = (uint64_t)blockIdx.x * kMsWarps + (threadIdx.x >> 5);
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t items = (m + 31) / 32 * G;
+  uint32_t* const f0 = a.fl[0];
+  uint32_t* const f1 = a.fl[1];
+  uint32_t* const f2 = a.fl[2];
+  for (uint64_t bt = a.b_begin; bt < a.b_end; bt++) {
+    const uint64_t s0 = bt * S;
+    const uint64_t left = a.n_sources - s0;
+    const uint32_t k = left < S ? (uint32_t)left : (uint32_t)S;
+    for (uint64_t x = gtid; x < n * S; x += nthreads) a.dist[x] = kWsInf;
+    for (uint64_t x = gtid; x < n * G; x += nthreads) {
+      f0[x] = 0;
+      f1[x] = 0;
+      f2[x] = 0;
+    }
+    grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+    if (*(volatile int*)a.err) return;
+    if (blockIdx.x == 0) {
+      if (threadIdx.x < 3) a.count[threadIdx.x] = 0;
+      if (threadIdx.x < k) {
+        const uint32_t src = a.sources[s0 + threadIdx.x];
+        a.dist[(uint64_t)src * S + threadIdx.x] = 0;  // +0.0
+        atomicOr(&f0[(uint64_t)src * G + (threadIdx.x >> 5)], 1u << (threadIdx.x & 31));
+      }
+    }
+    grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+    if (*(volatile int*)a.err) return;
+    for (uint32_t round = 0;; round++) {
+      const uint32_t r3 = round % 3;
+      const uint32_t* cur = r3 == 0 ? f0 : (r3 == 1 ? f1 : f2);
+      uint32_t* nxt = r3 == 0 ? f1 : (r3 == 1 ? f2 : f0);
+      uint32_t* clr = r3 == 0 ? f2 : (r3 == 1 ? f0 : f1);  // read two rounds ago, set next round
+      if (threadIdx.x == 0) s_any = 0;
+      // counter (round + 1) % 3 was last read before the previous barrier
+      if (blockIdx.x == 0 && threadIdx.x == 0) a.count[(round + 1) % 3] = 0;
+      for (uint64_t x = gtid; x < n * G; x += nthreads) clr[x] = 0;
+      __syncthreads();
+      bool lowered = false;
+      for (uint64_t item = gwarp; item < items; item += nwarps) {
+        const uint64_t sub = item % G;
+        const uint64_t e = item / G * 32 + lane;
+        uint32_t v = 0, w = 0, c = 0;
+        double x = 0.0;
+        if (e < m) {
+          v = __ldg(&a.esrc[e]);
+          c = __ldcg(&cur[(uint64_t)v * G + sub]);
+          if (c) {
+            w = __ldg(&a.tgt[e]);
+            x = __ldg(&a.wt[e]);
+          }
+        }
+        unsigned act = __ballot_sync(0xffffffffu, c != 0);
+        const uint64_t col = sub * 32 + lane;
+        while (act) {
+          const int j = __ffs(act) - 1;
+          act &= act - 1;
+          const uint32_t vj = __shfl_sync(0xffffffffu, v, j), wj = __shfl_sync(0xffffffffu, w, j);
+          const uint32_t cj = __shfl_sync(0xffffffffu, c, j);
+          const double xj = __shfl_sync(0xffffffffu, x, j);
+          bool imp = false;
+          if ((cj >> lane) & 1u) {
+            const double dv = __longlong_as_double((long long)__ldcg(&a.dist[(uint64_t)vj * S + col]));
+            const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(dv, xj));
+            unsigned long long* p = &a.dist[(uint64_t)wj * S + col];
+            if (nd < __ldcg(p)) imp = atomicMin(p, nd) > nd;
+          }
+          const unsigned b = __ballot_sync(0xffffffffu, imp);
+          if (b) {
+            lowered = true;
+            if (lane == 0) atomicOr(&nxt[(uint64_t)wj * G + sub], b);
+          }
+        }
+      }
+      if (lowered) s_any = 1;
+      __syncthreads();
+      if (threadIdx.x == 0 && s_any) atomicAdd(&a.count[r3], 1ull);
+      grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+      if (*(volatile int*)a.err) return;
+      const bool more = __ldcg(&a.count[r3]) != 0;
+      __syncthreads();
+      if (!more) break;
+    }
+    // node-order folds (closeness.rs:196-223), one lane per source
+    for (uint64_t sub = gwarp; sub < G; sub += nwarps) {
+      const uint64_t col = sub * 32 + lane;
+      if (col < k) {
+        const uint32_t u = a.sources[s0 + col];
+        double sum = 0.0;
+        long long reach = 0;
+#pragma unroll 8
+        for (uint64_t v = 0; v < n; v++) {
+          const unsigned long long bits = __ldcg(&a.dist[v * S + col]);
+          if (v != u && bits < kWsInf) {  // finite (no NaN reaches a distance)
+            sum = __dadd_rn(sum, __longlong_as_double((long long)bits));
+            reach++;
+          }
+        }
+        a.out[s0 + col] = sum > 0.0 ? (double)reach / sum : 0.0;
+      }
+    }
+    // the next batch rewrites dist: every fold must be done
+    grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+    if (*(volatile int*)a.err) return;
+  }
+}
+
+__global__ void ws_slot_src_k(const uint32_t* __restrict__ off, uint64_t n, uint64_t m, uint32_t* esrc) {
+  for_each_slot_owner(off, n, m, [&](uint64_t k, uint32_t u) { esrc[k] = u; });
+}
+
 __global__ void ms_iota_k(uint32_t* out, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x)
@@ -523,6 +676,66 @@ static std::vector<uint32_t> stats_sources(uint64_t n, int has_frac, double frac
   return out;
 }
 
+// Weighted closeness of every node into d_out (enqueued on s, returns after
+// completion).  d_w: edge weights by original edge row (device).
+static void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_out, cudaStream_t s) {
+  const uint64_t n = t->n;
+  DirView dv = dir_view(t, 0, s);
+  DirWeights dw;
+  gather_dir_weights(t, dv, d_w, dw, s);
+  uint64_t G = kWsDistBudget / (n * 256);
+  G = G < 1 ? 1 : (G > 8 ? 8 : G);
+  const uint64_t S = 32 * G;
+  const uint64_t m = t->m;
+  Scratch<unsigned long long> dist(n * S, s), count(3, s);
+  Scratch<uint32_t> fa(n * G, s), fb(n * G, s), fc(n * G, s), src(n, s), esrc(m ? m : 1, s);
+  if (m) {
+    ws_slot_src_k<<<grid_for(m, kBlock, 148u * 64u), kBlock, 0, s>>>(dv.off0, n, m, esrc.get());
+    UG_LAUNCH_CHECK();
+  }
+  Scratch<unsigned> ctl(4, s);
+  UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
+  ms_iota_k<<<grid_for(n), kBlock, 0, s>>>(src.get(), n);
+  UG_LAUNCH_CHECK();
+  int per_sm = 0;
+  UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ws_persist_k, kMsBlock, 0));
+  UG_CHECK(per_sm > 0, URSA_GPU_ECUDA, "closeness_weighted: kernel cannot be resident");
+  const uint64_t want = ((m + 31) / 32 * G + kMsWarps - 1) / kMsWarps;  // a warp per (chunk, sub-row)
+  const uint64_t cap = (uint64_t)per_sm * sm_count(t->device);
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
+  WsArgs a;
+  a.off = dv.off0;
+  a.tgt = dv.tgt0;
+  a.esrc = esrc.get();
+  a.wt = dw.w0.get();
+  a.n = n;
+  a.m = m;
+  a.sources = src.get();
+  a.n_sources = n;
+  a.G = (unsigned)G;
+  a.dist = dist.get();
+  a.fl[0] = fa.get();
+  a.fl[1] = fb.get();
+  a.fl[2] = fc.get();
+  a.count = count.get();
+  a.out = d_out;
+  a.bar = ctl.get();
+  a.err = (int*)(ctl.get() + 2);
+  const uint64_t batches = (n + S - 1) / S;
+  const uint64_t per_launch = std::max<uint64_t>(1, kMsSourcesPerLaunch / S);
+  for (uint64_t b = 0; b < batches; b += per_launch) {
+    a.b_begin = b;
+    a.b_end = std::min(batches, b + per_launch);
+    void* args[] = {&a};
+    UG_CUDA(cudaLaunchCooperativeKernel((void*)ws_persist_k, dim3(grid), dim3(kMsBlock), args, 0, s));
+    count_launch();
+  }
+  int err = 0;
+  UG_CUDA(cudaMemcpyAsync(&err, ctl.get() + 2, 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  UG_CHECK(err == 0, URSA_GPU_ETIMEOUT, "closeness_weighted: a grid barrier wait expired");
+}
+
 }  // namespace ug
 
 using namespace ug;
@@ -563,28 +776,16 @@ int ursa_gpu_closeness_weighted(ursa_gpu_topo* t, const double* weights, uint64_
     UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
+    check_sssp_weights(weights, ti->m);
     const uint64_t n = ti->n;
     if (n == 0) return;
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);
-    Scratch<double> dw(ti->m ? ti->m : 1, s), dd(n, s);
+    Scratch<double> dw(ti->m ? ti->m : 1, s), d_out(n, s);
     if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
-    std::vector<double> dist(n);
-    for (uint64_t u = 0; u < n; u++) {
-      // exact f64 distances on the device (sssp.cu), then the reference's
-      // node-order f64 fold (closeness.rs:196-223) on the host
-      dijkstra_run(ti, dw.get(), (uint32_t)u, 0, dd.get(), s);
-      UG_CUDA(cudaMemcpyAsync(dist.data(), dd.get(), n * 8, cudaMemcpyDeviceToHost, s));
-      UG_CUDA(cudaStreamSynchronize(s));
-      double sum = 0.0;
-      int64_t reachable = 0;
-      for (uint64_t v = 0; v < n; v++)
-        if (v != u && std::isfinite(dist[v])) {
-          sum += dist[v];
-          reachable++;
-        }
-      out[u] = sum > 0.0 ? (double)reachable / sum : 0.0;
-    }
+    closeness_weighted_device(ti, dw.get(), d_out.get(), s);
+    UG_CUDA(cudaMemcpyAsync(out, d_out.get(), n * 8, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
   });
 }
 

@@ -341,6 +341,7 @@ int ursa_gpu_dijkstra_distances(ursa_gpu_topo* t, const double* weights, uint64_
     UG_CHECK(dir >= 0 && dir <= 2, URSA_GPU_EINVAL, "direction must be 0, 1 or 2");
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
+    check_sssp_weights(weights, ti->m);
     if (ti->n == 0) return;
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);
@@ -362,6 +363,7 @@ int ursa_gpu_shortest_path_weighted_with_cost(ursa_gpu_topo* t, const double* we
     *len = -1;
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
+    check_sssp_weights(weights, ti->m);
     cudaStream_t s = thread_stream(ti->device);
     Scratch<double> dw(ti->m ? ti->m : 1, s);
     if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
