@@ -402,11 +402,15 @@ void ms_launch(MsArgs a, uint64_t n_sources, int device, cudaStream_t s) {
 // read two rounds before.  Rounds end when one lowers nothing.
 // The fixpoint is Dijkstra's: dist[v] = min over in-edges of fl(dist[u] + x),
 // the minimum left-to-right f64 path sum (fl(a + x) is monotone in a and
-// >= a for x >= 0).  Each lane then folds its source's distances in node
-// order exactly as closeness_weighted does (f64 sum over reachable v != u).
+// >= a for x >= 0).  A launch relaxes up to R batches, each into its own
+// slot of a distance ring, then every warp of the grid folds one (batch,
+// sub-row): each lane sums its source's distances in node order exactly as
+// closeness_weighted does (f64 sum over reachable v != u), 16 loads ahead of
+// its adds -- the sums are sequential, so many sources fold at once.
 
 constexpr unsigned long long kWsInf = 0x7FF0000000000000ull;
 constexpr uint64_t kWsDistBudget = 64ull << 20;  // distance rows of one batch: stay in L2
+constexpr uint64_t kWsRingBudget = 2ull << 30;   // distance slots of one launch
 
 struct WsArgs {
   const uint32_t* off;   // out-CSR
@@ -418,7 +422,7 @@ struct WsArgs {
   uint64_t n_sources;
   uint64_t b_begin, b_end;  // batches of 32 G sources run by this launch
   unsigned G;
-  unsigned long long* dist;  // n x 32 G
+  unsigned long long* dist;  // ring: one n x 32 G slot per batch of the launch
   uint32_t* fl[3];           // n x G flags each; round r reads fl[r % 3]
   unsigned long long* count;  // 3 counters, index round % 3: blocks that lowered a distance
   double* out;               // closeness per source
@@ -442,7 +446,8 @@ __global__ void __launch_bounds__(kMsBlock) ws_persist_k(WsArgs a) {
     const uint64_t s0 = bt * S;
     const uint64_t left = a.n_sources - s0;
     const uint32_t k = left < S ? (uint32_t)left : (uint32_t)S;
-    for (uint64_t x = gtid; x < n * S; x += nthreads) a.dist[x] = kWsInf;
+    unsigned long long* const dist = a.dist + (bt - a.b_begin) * n * S;
+    for (uint64_t x = gtid; x < n * S; x += nthreads) dist[x] = kWsInf;
     for (uint64_t x = gtid; x < n * G; x += nthreads) {
       f0[x] = 0;
       f1[x] = 0;
@@ -454,7 +459,7 @@ __global__ void __launch_bounds__(kMsBlock) ws_persist_k(WsArgs a) {
       if (threadIdx.x < 3) a.count[threadIdx.x] = 0;
       if (threadIdx.x < k) {
         const uint32_t src = a.sources[s0 + threadIdx.x];
-        a.dist[(uint64_t)src * S + threadIdx.x] = 0;  // +0.0
+        dist[(uint64_t)src * S + threadIdx.x] = 0;  // +0.0
         atomicOr(&f0[(uint64_t)src * G + (threadIdx.x >> 5)], 1u << (threadIdx.x & 31));
       }
     }
@@ -494,9 +499,9 @@ __global__ void __launch_bounds__(kMsBlock) ws_persist_k(WsArgs a) {
           const double xj = __shfl_sync(0xffffffffu, x, j);
           bool imp = false;
           if ((cj >> lane) & 1u) {
-            const double dv = __longlong_as_double((long long)__ldcg(&a.dist[(uint64_t)vj * S + col]));
+            const double dv = __longlong_as_double((long long)__ldcg(&dist[(uint64_t)vj * S + col]));
             const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(dv, xj));
-            unsigned long long* p = &a.dist[(uint64_t)wj * S + col];
+            unsigned long long* p = &dist[(uint64_t)wj * S + col];
             if (nd < __ldcg(p)) imp = atomicMin(p, nd) > nd;
           }
           const unsigned b = __ballot_sync(0xffffffffu, imp);
@@ -515,27 +520,39 @@ __global__ void __launch_bounds__(kMsBlock) ws_persist_k(WsArgs a) {
       __syncthreads();
       if (!more) break;
     }
-    // node-order folds (closeness.rs:196-223), one lane per source
-    for (uint64_t sub = gwarp; sub < G; sub += nwarps) {
-      const uint64_t col = sub * 32 + lane;
-      if (col < k) {
-        const uint32_t u = a.sources[s0 + col];
-        double sum = 0.0;
-        long long reach = 0;
-#pragma unroll 8
-        for (uint64_t v = 0; v < n; v++) {
-          const unsigned long long bits = __ldcg(&a.dist[v * S + col]);
-          if (v != u && bits < kWsInf) {  // finite (no NaN reaches a distance)
-            sum = __dadd_rn(sum, __longlong_as_double((long long)bits));
-            reach++;
-          }
+  }
+  // every batch's relaxations ended at a barrier: fold the launch's batches,
+  // one (batch, sub-row) per warp (closeness.rs:196-223)
+  const uint64_t nb = a.b_end - a.b_begin;
+  for (uint64_t item = gwarp; item < nb * G; item += nwarps) {
+    const uint64_t slot = item / G, sub = item % G;
+    const uint64_t s0 = (a.b_begin + slot) * S;
+    const uint64_t col = sub * 32 + lane;
+    if (s0 + col >= a.n_sources) continue;
+    const uint32_t u = a.sources[s0 + col];
+    const unsigned long long* const base = a.dist + slot * n * S + col;
+    double sum = 0.0;
+    long long reach = 0;
+    uint64_t v = 0;
+    for (; v + 16 <= n; v += 16) {
+      unsigned long long b[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) b[i] = __ldcg(base + (v + i) * S);
+#pragma unroll
+      for (int i = 0; i < 16; i++)
+        if (v + i != u && b[i] < kWsInf) {  // finite (no NaN reaches a distance)
+          sum = __dadd_rn(sum, __longlong_as_double((long long)b[i]));
+          reach++;
         }
-        a.out[s0 + col] = sum > 0.0 ? (double)reach / sum : 0.0;
+    }
+    for (; v < n; v++) {
+      const unsigned long long bits = __ldcg(base + v * S);
+      if (v != u && bits < kWsInf) {
+        sum = __dadd_rn(sum, __longlong_as_double((long long)bits));
+        reach++;
       }
     }
-    // the next batch rewrites dist: every fold must be done
-    grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
-    if (*(volatile int*)a.err) return;
+    a.out[s0 + col] = sum > 0.0 ? (double)reach / sum : 0.0;
   }
 }
 
@@ -687,7 +704,10 @@ static void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_
   G = G < 1 ? 1 : (G > 8 ? 8 : G);
   const uint64_t S = 32 * G;
   const uint64_t m = t->m;
-  Scratch<unsigned long long> dist(n * S, s), count(3, s);
+  const uint64_t batches = (n + S - 1) / S;
+  uint64_t R = kWsRingBudget / (n * S * 8);
+  R = std::max<uint64_t>(1, std::min<uint64_t>(R, std::min<uint64_t>(64, batches)));
+  Scratch<unsigned long long> dist(R * n * S, s), count(3, s);
   Scratch<uint32_t> fa(n * G, s), fb(n * G, s), fc(n * G, s), src(n, s), esrc(m ? m : 1, s);
   if (m) {
     ws_slot_src_k<<<grid_for(m, kBlock, 148u * 64u), kBlock, 0, s>>>(dv.off0, n, m, esrc.get());
@@ -721,11 +741,9 @@ static void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_
   a.out = d_out;
   a.bar = ctl.get();
   a.err = (int*)(ctl.get() + 2);
-  const uint64_t batches = (n + S - 1) / S;
-  const uint64_t per_launch = std::max<uint64_t>(1, kMsSourcesPerLaunch / S);
-  for (uint64_t b = 0; b < batches; b += per_launch) {
+  for (uint64_t b = 0; b < batches; b += R) {
     a.b_begin = b;
-    a.b_end = std::min(batches, b + per_launch);
+    a.b_end = std::min(batches, b + R);
     void* args[] = {&a};
     UG_CUDA(cudaLaunchCooperativeKernel((void*)ws_persist_k, dim3(grid), dim3(kMsBlock), args, 0, s));
     count_launch();
