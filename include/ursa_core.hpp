@@ -8,7 +8,9 @@
 // kernel functions degree, pagerank, pagerank_weighted, bfs_distances,
 // shortest_path, dijkstra_distances, shortest_path_weighted[_with_cost],
 // k_hop, connected_components_weak, triangle_count, clustering_coefficient,
-// betweenness and betweenness_weighted.  Vec<T> becomes std::vector<T>,
+// betweenness, betweenness_weighted, closeness and closeness_weighted
+// (algo/closeness.rs:69-224), plus ursa-plan's avg_path_length and diameter
+// (ursa-plan/src/stats.rs:142-167).  Vec<T> becomes std::vector<T>,
 // Option<T> becomes std::optional<T>.  Where the Rust code would panic (a
 // contract violation, e.g. a weights length that is not the edge count), the
 // mirror throws ursa_core::Error carrying the C ABI status and message.
@@ -214,6 +216,30 @@ inline std::vector<double> betweenness_weighted(const Topology& t, const std::ve
                                       sample.has_value(), sample.value_or(0.0), seed.has_value(),
                                       seed.value_or(0), out.data()));
   return out;
+}
+
+inline std::vector<double> closeness(const Topology& t) {
+  std::vector<double> out(t.n_nodes());
+  check(ursa_gpu_closeness(t.handle(), out.data()));
+  return out;
+}
+
+inline std::vector<double> closeness_weighted(const Topology& t, const std::vector<double>& weights) {
+  std::vector<double> out(t.n_nodes());
+  check(ursa_gpu_closeness_weighted(t.handle(), weights.data(), weights.size(), out.data()));
+  return out;
+}
+
+inline double avg_path_length(const Topology& t, std::optional<double> sample) {
+  double v = 0.0;
+  check(ursa_gpu_avg_path_length(t.handle(), sample.has_value(), sample.value_or(0.0), &v));
+  return v;
+}
+
+inline int64_t diameter(const Topology& t, bool approximate) {
+  int64_t d = 0;
+  check(ursa_gpu_diameter(t.handle(), approximate ? 1 : 0, &d));
+  return d;
 }
 
 }  // namespace algo

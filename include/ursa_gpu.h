@@ -451,6 +451,113 @@ int ursa_gpu_server_result(ursa_gpu_server *s, uint64_t ticket, ursa_gpu_query_i
                            void *out, uint64_t cap_elems);
 int ursa_gpu_server_get_stats(ursa_gpu_server *s, ursa_gpu_server_stats *stats);
 
+/* ------------------------------------------------------------------------
+ * Arrow results: the "Arrow arrays out" half of the operator
+ * (ursa-plan/src/result.rs:144-261).
+ *
+ * query_batch computes every requested column on the device into one staging
+ * block laid out as Arrow value buffers, translates the id column (or the
+ * hop / path endpoints) dense -> user on the device, and copies the block to
+ * pinned host memory once.  The result exports as an Arrow C Data Interface
+ * struct array (one RecordBatch): its buffers point into that pinned block,
+ * so a consumer (arrow-rs FFI_ArrowArray, pyarrow _import_from_c) takes the
+ * columns without another copy; the block lives until the result and every
+ * export of it are released.  Without an IdMap (ids == NULL) the id columns
+ * are the dense UInt32 node indices.
+ * ------------------------------------------------------------------------ */
+
+/* The Arrow C Data Interface structures, as the Arrow specification defines
+ * them (skipped if the consumer's Arrow headers already did). */
+#ifndef ARROW_C_DATA_INTERFACE
+#define ARROW_C_DATA_INTERFACE
+#define ARROW_FLAG_DICTIONARY_ORDERED 1
+#define ARROW_FLAG_NULLABLE 2
+#define ARROW_FLAG_MAP_KEYS_SORTED 4
+struct ArrowSchema {
+  const char *format;
+  const char *name;
+  const char *metadata;
+  int64_t flags;
+  int64_t n_children;
+  struct ArrowSchema **children;
+  struct ArrowSchema *dictionary;
+  void (*release)(struct ArrowSchema *);
+  void *private_data;
+};
+struct ArrowArray {
+  int64_t length;
+  int64_t null_count;
+  int64_t offset;
+  int64_t n_buffers;
+  int64_t n_children;
+  const void **buffers;
+  struct ArrowArray **children;
+  struct ArrowArray *dictionary;
+  void (*release)(struct ArrowArray *);
+  void *private_data;
+};
+#endif
+
+typedef struct ursa_gpu_result ursa_gpu_result;
+
+/* GraphAlgo (ursa-plan/src/logical.rs:37-65). */
+enum {
+  URSA_GPU_ALGO_PAGERANK = 0,
+  URSA_GPU_ALGO_CONNECTED_COMPONENTS = 1,
+  URSA_GPU_ALGO_DEGREE = 2,
+  URSA_GPU_ALGO_TRIANGLE_COUNT = 3,
+  URSA_GPU_ALGO_CLUSTERING_COEFFICIENT = 4,
+  URSA_GPU_ALGO_BETWEENNESS = 5,
+  URSA_GPU_ALGO_CLOSENESS = 6,
+  URSA_GPU_ALGO_LABEL_PROPAGATION = 7, /* host-side kernel: URSA_GPU_EINVAL here */
+  URSA_GPU_ALGO_LOUVAIN = 8            /* host-side kernel: URSA_GPU_EINVAL here */
+};
+
+/* OutputColumn::Algo (result.rs:28-35; value types result.rs:52-63): a
+ * named node-valued column.  Only the fields of `algo` are read.  weights:
+ * n_edges f64 by edge row (host), or NULL; present for pagerank, betweenness
+ * and closeness (their weighted forms).  Strong components (strong != 0)
+ * run on the host: URSA_GPU_EINVAL. */
+typedef struct {
+  const char *name;
+  int algo;
+  double damping;    /* PAGERANK */
+  uint32_t max_iter; /* PAGERANK */
+  double tol;        /* PAGERANK */
+  int strong;        /* CONNECTED_COMPONENTS */
+  int direction;     /* DEGREE: 0 out, 1 in, 2 both */
+  int has_sample;    /* BETWEENNESS */
+  double sample;
+  int has_seed;
+  uint64_t seed;
+  const double *weights;
+  uint64_t n_weights;
+} ursa_gpu_output_column;
+
+/* query_schema + query_batch (result.rs:144-168): columns ("id", name_1,
+ * ...), n_nodes rows; id is Int64 (the IdMap's user ids) or UInt32; Float64
+ * for pagerank, clustering, closeness and betweenness, UInt32 otherwise; none
+ * nullable.  ids, when given, must hold exactly the topology's nodes. */
+int ursa_gpu_query_batch(ursa_gpu_topo *t, ursa_gpu_idmap *ids, const ursa_gpu_output_column *cols,
+                         uint64_t n_cols, ursa_gpu_result **out);
+/* hop_schema + hop_batch (result.rs:171-199): ("src", "dst") = (seed,
+ * reached) per k_hop pair, in k_hop's order. */
+int ursa_gpu_hop_batch(ursa_gpu_topo *t, ursa_gpu_idmap *ids, const uint32_t *seeds,
+                       uint64_t n_seeds, uint32_t k, int dir, ursa_gpu_result **out);
+/* path_schema + path_batch (result.rs:203-261): ("src", "dst", "hop" Int64,
+ * "cost" Float64), one row per path edge; cost = the settled distance of the
+ * edge's destination (weights given) or hop + 1.  No row for an unreachable
+ * target or a one-node path. */
+int ursa_gpu_path_batch(ursa_gpu_topo *t, ursa_gpu_idmap *ids, uint32_t source, uint32_t target,
+                        int dir, const double *weights, uint64_t n_weights, ursa_gpu_result **out);
+uint64_t ursa_gpu_result_num_rows(const ursa_gpu_result *r);
+uint64_t ursa_gpu_result_num_columns(const ursa_gpu_result *r);
+/* Exports the result as a struct array and its schema (format "+s", one
+ * child per column).  The consumer calls each structure's release. */
+int ursa_gpu_result_export(ursa_gpu_result *r, struct ArrowSchema *schema, struct ArrowArray *array);
+/* Drops the caller's reference; exported arrays keep the block alive. */
+void ursa_gpu_result_free(ursa_gpu_result *r);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,14 @@ int main() {
   auto bc = algo::betweenness(Topology::build(5, {0, 1, 2, 3}, {1, 2, 3, 4}), std::nullopt,
                               std::nullopt);
   EXPECT(bc == std::vector<double>({0.0, 3.0, 4.0, 3.0, 0.0}));
+  // closeness.rs:244-252 (directed line), stats.rs (directed triangle)
+  EXPECT(algo::closeness(Topology::build(4, {0, 1, 2}, {1, 2, 3})) ==
+         std::vector<double>({0.5, 2.0 / 3.0, 1.0, 0.0}));
+  auto cw = algo::closeness_weighted(Topology::build(3, {0, 1, 0}, {1, 2, 2}), {1.0, 1.0, 5.0});
+  EXPECT(std::fabs(cw[0] - 2.0 / 3.0) < 1e-12 && std::fabs(cw[1] - 1.0) < 1e-12);
+  Topology tri = Topology::build(3, {0, 1, 2}, {1, 2, 0});
+  EXPECT(algo::avg_path_length(tri, std::nullopt) == 1.5);
+  EXPECT(algo::diameter(tri, false) == 2);
   // contract violation -> Error (the Rust code asserts)
   bool threw = false;
   try {

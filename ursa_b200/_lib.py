@@ -182,6 +182,13 @@ SIGNATURES = {
     "ursa_gpu_idmap_dense_edges": (i32, [P, P, P]),
     "ursa_gpu_idmap_topology": (i32, [P, C.POINTER(P)]),
     "ursa_gpu_idmap_gather_user": (i32, [P, P, u64, P]),
+    "ursa_gpu_query_batch": (i32, [P, P, P, u64, P]),
+    "ursa_gpu_hop_batch": (i32, [P, P, P, u64, u32, i32, P]),
+    "ursa_gpu_path_batch": (i32, [P, P, u32, u32, i32, P, u64, P]),
+    "ursa_gpu_result_num_rows": (u64, [P]),
+    "ursa_gpu_result_num_columns": (u64, [P]),
+    "ursa_gpu_result_export": (i32, [P, P, P]),
+    "ursa_gpu_result_free": (None, [P]),
     "ursa_gpu_idmap_lookup": (i32, [P, P, u64, P, P]),
     "ursa_gpu_server_create": (i32, [P, C.POINTER(ServerConfig), C.POINTER(P)]),
     "ursa_gpu_server_destroy": (None, [P]),

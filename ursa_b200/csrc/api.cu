@@ -11,9 +11,6 @@
 
 namespace ug {
 
-void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* d_weights,
-                  double* d_out, cudaStream_t s, ursa_gpu_pagerank_stats* stats);
-
 namespace {
 thread_local std::string g_last_error;
 thread_local int g_device = 0;
@@ -53,6 +50,16 @@ __global__ void check_range_k(const uint32_t* __restrict__ a, const uint32_t* __
     if ((uint64_t)a[i] >= n || (uint64_t)b[i] >= n) atomicOr(bad, 1u);
 }
 }  // namespace
+
+// degree.rs:12-30: out-, in- or total degree per node.
+void degree_run(TopoImpl* t, int dir, uint32_t* d_out, cudaStream_t s) {
+  if (t->n == 0) return;
+  if (dir != 0) ensure_in(t, s);
+  const uint32_t* a = dir == 1 ? t->in.off.get() : t->out.off.get();
+  const uint32_t* b = dir == 2 ? t->in.off.get() : nullptr;
+  degree_dir_k<<<grid_for(t->n), kBlock, 0, s>>>(a, b, t->n, d_out);
+  UG_LAUNCH_CHECK();
+}
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -287,12 +294,8 @@ int ursa_gpu_degree(ursa_gpu_topo* t, int dir, uint32_t* out) {
     if (ti->n == 0) return;
     require(out, "out");
     cudaStream_t s = call_stream(ti, nullptr);
-    if (dir != 0) ensure_in(ti, s);
     Scratch<uint32_t> d(ti->n, s);
-    const uint32_t* a = dir == 1 ? ti->in.off.get() : ti->out.off.get();
-    const uint32_t* b = dir == 2 ? ti->in.off.get() : nullptr;
-    degree_dir_k<<<grid_for(ti->n), kBlock, 0, s>>>(a, b, ti->n, d.get());
-    UG_LAUNCH_CHECK();
+    degree_run(ti, dir, d.get(), s);
     UG_CUDA(cudaMemcpyAsync(out, d.get(), ti->n * 4, cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));
   });

@@ -314,10 +314,6 @@ void bfs_distances_run(TopoImpl* t, uint32_t source, int dir, int32_t* d_dist, c
 }
 
 // ------------------------------------------------------------------- k_hop
-struct PairsHost {
-  std::vector<uint32_t> seeds, reached;
-};
-
 void k_hop_run(TopoImpl* t, const uint32_t* seeds, uint64_t n_seeds, uint32_t k, int dir,
                PairsHost& out, cudaStream_t s) {
   const uint64_t n = t->n;

@@ -162,6 +162,50 @@ struct ursa_gpu_idmap {
   uint32_t special_dense = 0xFFFFFFFFu;
 };
 
+namespace ug {
+
+namespace {
+
+// IdMap::gather_user (id_map.rs:381-396): out[i] = to_user[dense[i]]; an
+// index past the map (the reference's slice index would panic) sets *bad.
+__global__ void gather_user_k(const int64_t* __restrict__ to_user, uint64_t n_ids,
+                              const uint32_t* __restrict__ dense, uint64_t n, int64_t* __restrict__ out,
+                              unsigned* __restrict__ bad) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = dense[i];
+    if (d < n_ids) {
+      out[i] = to_user[d];
+    } else {
+      out[i] = 0;
+      *bad = 1u;
+    }
+  }
+}
+
+}  // namespace
+
+const int64_t* idmap_users(ursa_gpu_idmap* m, uint64_t* n_ids, int* device) {
+  *n_ids = m->n_ids;
+  *device = m->device;
+  return m->to_user.get();
+}
+
+void idmap_gather_device(ursa_gpu_idmap* m, const uint32_t* d_dense, uint64_t n, int64_t* d_out,
+                         cudaStream_t s) {
+  if (n == 0) return;
+  Scratch<unsigned> bad(1, s);
+  UG_CUDA(cudaMemsetAsync(bad.get(), 0, 4, s));
+  gather_user_k<<<grid_for(n), kBlock, 0, s>>>(m->to_user.get(), m->n_ids, d_dense, n, d_out, bad.get());
+  UG_LAUNCH_CHECK();
+  unsigned h = 0;
+  UG_CUDA(cudaMemcpyAsync(&h, bad.get(), 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  UG_CHECK(h == 0, URSA_GPU_EINVAL, "gather_user: dense index out of range");
+}
+
+}  // namespace ug
+
 extern "C" {
 
 int ursa_gpu_idmap_build(uint64_t n_chunks, const int64_t* const* src_chunks,
@@ -306,15 +350,13 @@ int ursa_gpu_idmap_gather_user(ursa_gpu_idmap* m, const uint32_t* dense, uint64_
     UG_CHECK(m, URSA_GPU_EINVAL, "idmap is NULL");
     if (!n) return;
     UG_CHECK(dense && out, URSA_GPU_EINVAL, "dense / out is NULL");
-    std::vector<int64_t> users(m->n_ids);
     cudaStream_t s = thread_stream(m->device);
-    if (m->n_ids)
-      UG_CUDA(cudaMemcpyAsync(users.data(), m->to_user.get(), m->n_ids * 8, cudaMemcpyDeviceToHost, s));
+    Scratch<uint32_t> d_dense(n, s);
+    Scratch<int64_t> d_out(n, s);
+    UG_CUDA(cudaMemcpyAsync(d_dense.get(), dense, n * 4, cudaMemcpyHostToDevice, s));
+    idmap_gather_device(m, d_dense.get(), n, d_out.get(), s);
+    UG_CUDA(cudaMemcpyAsync(out, d_out.get(), n * 8, cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));
-    for (uint64_t i = 0; i < n; i++) {
-      UG_CHECK(dense[i] < m->n_ids, URSA_GPU_EINVAL, "gather_user: dense index out of range");
-      out[i] = users[dense[i]];
-    }
   });
 }
 

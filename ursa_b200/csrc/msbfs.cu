@@ -641,7 +641,7 @@ void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_
 
 // Closeness of every node into the device array d_out, enqueued on s;
 // returns after completion, with the device time of the enqueued work.
-static void closeness_device(TopoImpl* t, double* d_out, cudaStream_t s, float* device_ms) {
+void closeness_device(TopoImpl* t, double* d_out, cudaStream_t s, float* device_ms) {
   const uint64_t n = t->n;
   Scratch<unsigned long long> d_reach(n, s), d_dsum(n, s);
   Scratch<uint32_t> d_maxd(n, s), d_src(n, s);
@@ -695,7 +695,7 @@ static std::vector<uint32_t> stats_sources(uint64_t n, int has_frac, double frac
 
 // Weighted closeness of every node into d_out (enqueued on s, returns after
 // completion).  d_w: edge weights by original edge row (device).
-static void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_out, cudaStream_t s) {
+void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_out, cudaStream_t s) {
   const uint64_t n = t->n;
   DirView dv = dir_view(t, 0, s);
   DirWeights dw;

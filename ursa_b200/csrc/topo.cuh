@@ -7,6 +7,8 @@
 // widens them to the reference's u64 on download.
 #pragma once
 
+#include <vector>
+
 #include <memory>
 #include <mutex>
 
@@ -64,6 +66,39 @@ TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_
 
 // Slot -> owning node for a CSR (binary search over offsets), n_slots = m.
 void csr_owners(const uint32_t* off, uint64_t n, uint64_t m, uint32_t* owner, cudaStream_t s);
+
+// Device-output forms of the kernels (each enqueued on s; results in device
+// arrays of n entries unless stated).  d_weights: n_edges f64 by edge row.
+void degree_run(TopoImpl* t, int dir, uint32_t* d_out, cudaStream_t s);
+void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* d_weights,
+                  double* d_out, cudaStream_t s, ursa_gpu_pagerank_stats* stats);
+void cc_weak_run(TopoImpl* t, uint32_t* d_out, cudaStream_t s);
+void triangle_count_run(TopoImpl* t, uint32_t* d_tri, cudaStream_t s);
+void clustering_run(TopoImpl* t, double* d_out, cudaStream_t s);
+void betweenness_run(TopoImpl* t, const double* d_weights, bool has_sample, double sample,
+                     bool has_seed, uint64_t seed, double* d_out, cudaStream_t s);
+void closeness_device(TopoImpl* t, double* d_out, cudaStream_t s, float* device_ms);
+void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_out, cudaStream_t s);
+
+// k_hop pairs (seed, reached) in the reference's emission order, on the host.
+struct PairsHost {
+  std::vector<uint32_t> seeds, reached;
+};
+void k_hop_run(TopoImpl* t, const uint32_t* seeds, uint64_t n_seeds, uint32_t k, int dir,
+               PairsHost& out, cudaStream_t s);
+// Paths into host buffers of cap entries: length, -1 if unreachable, or
+// -(length) - 2 if cap is too small.
+int64_t shortest_path_run(TopoImpl* t, uint32_t source, uint32_t target, int dir, uint32_t* path,
+                          uint64_t cap, cudaStream_t s);
+int64_t weighted_path_run(TopoImpl* t, const double* d_weights, uint32_t source, uint32_t target,
+                          int dir, uint32_t* path, double* costs, uint64_t cap, cudaStream_t s);
+
+// The IdMap's device user ids (dense order) and their count; gathers
+// d_out[i] = user id of d_dense[i] on the device (URSA_GPU_EINVAL if an index
+// is out of range).
+const int64_t* idmap_users(ursa_gpu_idmap* m, uint64_t* n_ids, int* device);
+void idmap_gather_device(ursa_gpu_idmap* m, const uint32_t* d_dense, uint64_t n, int64_t* d_out,
+                         cudaStream_t s);
 
 }  // namespace ug
 
