@@ -50,6 +50,9 @@ topology from the dense device columns.
 
 --workload closeness: all-source closeness on R-MAT-16 (65,536 nodes, edge
 factor 16, seed 2); GTEPS = n sources x m edges / time.
+
+--workload result: query_batch (id, degree, pagerank) on R-MAT-22 under
+Int64 user ids to a pyarrow RecordBatch, beside the per-column plain path.
 """
 
 from __future__ import annotations
@@ -531,6 +534,105 @@ def run_closeness(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+RESULT_WORKLOAD = "rmat22_query_batch_id_degree_pagerank"
+
+
+def run_result(args, rank, world):
+    """Arrow result materialisation (result.rs:160-168): query_batch of
+    (id, out-degree, pagerank d 0.85 tol 1e-6 max_iter 100) over R-MAT-22
+    under seeded random Int64 user ids, topology and IdMap resident, to a
+    pyarrow RecordBatch in host memory.  Beside it the plain path (the
+    per-column C-ABI calls into numpy, the host user-id array, and
+    RecordBatch.from_arrays) and an (id, degree) batch, whose time is nearly
+    all the copy path (id gather on the device, one D2H into pinned memory,
+    the zero-copy import)."""
+    import pyarrow as pa
+    import torch
+
+    local_rank = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    from ursa_b200 import _lib, algo
+    from ursa_b200.idmap import IdMap
+    from ursa_b200.result import OutputColumn, query_batch
+
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(local_rank))
+    n, s, d = make_workload()
+    label = np.random.default_rng(SEED).integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64)
+    ids = IdMap.from_edge_arrays(label[s], label[d])
+    topo = ids.topology()
+    topo.prepare(transpose=True)
+    rows = len(ids)
+    cols = [OutputColumn("deg", "degree", direction="out"),
+            OutputColumn("pr", "pagerank", damping=DAMPING, max_iter=MAX_ITER, tol=TOL)]
+    light = [OutputColumn("deg", "degree", direction="out")]
+
+    def timed(fn, k):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        ts = []
+        for _ in range(k):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts)
+
+    def plain():
+        deg = algo.degree(topo, "out")
+        pr = algo.pagerank(topo, damping=DAMPING, max_iter=MAX_ITER, tol=TOL)
+        return pa.RecordBatch.from_arrays([pa.array(ids.user_id_array()), pa.array(deg), pa.array(pr)],
+                                          names=["id", "deg", "pr"])
+
+    launches0 = L.ursa_gpu_launch_count()
+    t_query = timed(lambda: query_batch(topo, ids, cols), args.steps)
+    launches = (L.ursa_gpu_launch_count() - launches0) / (args.steps + max(args.warmup, 1))
+    t_light = timed(lambda: query_batch(topo, ids, light), args.steps)
+    t_plain = timed(plain, args.steps)
+    bytes_full = rows * (8 + 4 + 8)
+    bytes_light = rows * (8 + 4)
+    # the host link's own D2H rate into pinned memory for the same bytes
+    src_dev = torch.empty(bytes_light, dtype=torch.uint8, device="cuda")
+    dst_host = torch.empty(bytes_light, dtype=torch.uint8).pin_memory()
+    link = []
+    for _ in range(max(args.steps, 3)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dst_host.copy_(src_dev)
+        torch.cuda.synchronize()
+        link.append(time.perf_counter() - t0)
+    link_gbs = bytes_light / min(link) / 1e9
+    line = {
+        "metric": "query_batch_rows_per_s",
+        "value": rows / t_query,
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_query,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int64 ids, u32 degree, f64 ranks",
+        "data": "synthetic",
+        "config": {"workload": RESULT_WORKLOAD, "rows": rows, "n_edges": int(s.size),
+                   "columns": ["id", "deg", "pr"], "ids": "seeded uniform random int64 per R-MAT-22 node"},
+        "e2e": {"value": rows / t_query, "unit": "rows/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": bytes_full, "ms_per_step": 1e3 * t_query,
+                "note": "topology and IdMap resident; compute + id translation + one pinned D2H + import"},
+        "plain": {"value": rows / t_plain, "unit": "rows/s", "ms_per_step": 1e3 * t_plain,
+                  "note": "per-column C-ABI calls into numpy + host user ids + RecordBatch.from_arrays"},
+        "id_degree_batch": {"ms": 1e3 * t_light, "bytes": bytes_light,
+                            "gb_per_s": bytes_light / t_light / 1e9},
+        "roofline": {"bound": "host_link", "achieved": bytes_light / t_light / 1e9, "peak": link_gbs,
+                     "unit": "GB/s", "frac": link_gbs and (bytes_light / t_light / 1e9) / link_gbs,
+                     "peak_kind": "measured here: torch device-to-pinned copy of the same bytes",
+                     "traffic": None, "kernel": "(id, degree) query_batch end to end"},
+        "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 SERVE_WORKLOAD = "serve_rmat24_uploads"
 SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
 
@@ -924,7 +1026,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap", "closeness"])
+    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap", "closeness", "result"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids (defaults give the benchmark above)
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="pagerank max_iter (rmat22 workload)")
@@ -957,6 +1059,9 @@ def main():
         return
     if args.workload == "closeness":
         run_closeness(args, rank, world)
+        return
+    if args.workload == "result":
+        run_result(args, rank, world)
         return
 
     import torch

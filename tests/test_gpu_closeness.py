@@ -28,6 +28,13 @@ def _cases():
     out.append(("rmat11", n, s, d))
     chain = 130
     out.append(("chain130", chain, list(range(chain - 1)), list(range(1, chain))))  # 129 levels
+    # hubs: in-degree 2,499 and 1,200 (split scans over several warps), a
+    # tail leaving the hub, random edges among the spokes
+    rng = np.random.default_rng(12)
+    hs = list(range(1, 2500)) + list(range(1300, 2500)) + [0] + list(range(2500, 2599))
+    hd = [0] * 2499 + [1] * 1200 + [2500] + list(range(2501, 2600))
+    rs, rd = rng.integers(1, 2500, 3000), rng.integers(1, 2500, 3000)
+    out.append(("hubs", 2600, hs + rs.tolist(), hd + rd.tolist()))
     return out
 
 

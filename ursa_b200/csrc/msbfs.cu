@@ -12,8 +12,11 @@
 //   bottom-up otherwise: each w with sources still to find
 //   (need = active & ~visited[w]) ORs its in-neighbours' frontier masks,
 //   stopping as soon as every needed bit is found; new = acc & need.
-//   Nodes with at most 32 edges to scan are handled by one lane, heavier ones
-//   by the whole warp.  visited[w] |= new; next[w] = new.
+//   Nodes with at most 32 edges to scan are handled by one lane, up to
+//   kMsHub by the whole warp; a hub's in-edges are cut into kMsChunk-edge
+//   chunks that any warp takes, ORed into a per-hub accumulator and settled
+//   after one more barrier (one warp per hub put every other warp at the
+//   barrier waiting for it).  visited[w] |= new; next[w] = new.
 // A source that reached no new node on a level is finished and leaves the
 // active mask.  Per source, the number of nodes first reached on the level is
 // a column popcount of the new masks (one warp ballot per bit), summed per
@@ -41,6 +44,8 @@ constexpr int kMsWarps = kMsBlock / 32;
 constexpr uint64_t kMsSourcesPerLaunch = 1024;
 constexpr uint64_t kMsWaitNs = 5000000000ull;  // one grid-barrier wait
 constexpr uint64_t kMsPushDiv = 8;  // push while the frontier's out-edges are below m / 8
+constexpr uint32_t kMsHub = 512;    // in-degree above which a node's scan is split
+constexpr uint32_t kMsChunk = 512;  // in-edges per chunk of a split scan
 
 // W 64-bit words per node: bit j of word q belongs to source 64 q + j of the
 // batch.  A node's W words are contiguous (one 32-byte sector for W = 4).
@@ -135,6 +140,12 @@ struct MsArgs {
   unsigned long long* fr0;      // frontier masks, odd levels' input
   unsigned long long* fr1;      // even levels' input
   unsigned long long* acc;      // pushed masks of a top-down level; all zero between levels
+  const uint32_t* hubs;         // nodes with in-degree > kMsHub, ascending
+  uint64_t n_hubs;
+  const uint32_t* chunk_hub;    // per kMsChunk-edge chunk of a hub's in-edges: hub index,
+  const uint32_t* chunk_lo;     //   first in-CSR slot
+  uint64_t n_chunks;
+  unsigned long long* hacc;     // n_hubs x W: OR of a bottom-up level's chunk results; zero between levels
   unsigned long long* count;    // 3 rows of 64 W + 8, row = level % 3; [64 W] = frontier out-edges
   unsigned long long* reach;
   unsigned long long* dsum;
@@ -184,6 +195,72 @@ __device__ __forceinline__ void ms_push(const MsArgs& a, const unsigned long lon
       }
     }
   }
+}
+
+// Settles node w (lanes with valid) for this level: visited |= new,
+// next[w] = new, and adds the per-source counts and the new nodes'
+// out-edges to the block's tallies.  Every lane of the warp calls it.
+template <int W>
+__device__ __forceinline__ void ms_settle(const MsArgs& a, unsigned long long* nxt, uint64_t w, bool valid,
+                                          const Msk<W>& vis, const Msk<W>& nw, unsigned* sc,
+                                          unsigned long long* s_mf, int lane) {
+  unsigned long long od = 0;
+  const bool got = mk_any(nw);
+  if (valid) {
+    if (got) {
+      Msk<W> nv = vis;
+      mk_or(nv, nw);
+      mk_store<W>(a.visited, w, nv);
+      od = __ldg(&a.out_off[w + 1]) - __ldg(&a.out_off[w]);
+    }
+    mk_store<W>(nxt, w, nw);
+  }
+  if (__any_sync(0xffffffffu, got)) {
+#pragma unroll
+    for (int q = 0; q < W; q++) {
+      if (!__any_sync(0xffffffffu, nw.v[q] != 0)) continue;
+#pragma unroll 8
+      for (int b = 0; b < 64; b++) {
+        const unsigned c = __popc(__ballot_sync(0xffffffffu, (nw.v[q] >> b) & 1ull));
+        if (lane == 0 && c) atomicAdd(&sc[64 * q + b], c);
+      }
+    }
+    for (int o = 16; o; o >>= 1) od += __shfl_down_sync(0xffffffffu, od, o);
+    if (lane == 0) atomicAdd(s_mf, od);
+  }
+}
+
+// Bottom-up scan of one chunk of a hub's in-edges: ORs the frontier masks of
+// up to kMsChunk in-neighbours (stopping once every needed source is found)
+// into hacc of the hub.  One warp per chunk.
+template <int W>
+__device__ __forceinline__ void ms_hub_chunk(const MsArgs& a, const unsigned long long* cur,
+                                             const Msk<W>& active, uint64_t c, int lane) {
+  const uint32_t h = __ldg(&a.chunk_hub[c]);
+  const uint32_t w = __ldg(&a.hubs[h]);
+  const Msk<W> need = mk_andnot(active, mk_load<W>(a.visited, w));
+  if (!mk_any(need)) return;  // warp-uniform: one chunk per warp
+  const uint32_t e0 = __ldg(&a.chunk_lo[c]);
+  const uint32_t end = __ldg(&a.in_off[w + 1]);
+  const uint32_t e1 = end - e0 > kMsChunk ? e0 + kMsChunk : end;
+  Msk<W> acc = mk_zero<W>();
+  constexpr int U = W == 1 ? 4 : 2;  // in-edges per lane per step
+  for (uint32_t e = e0; e < e1; e += 32 * U) {
+    Msk<W> f = mk_zero<W>();
+#pragma unroll
+    for (int q = 0; q < U; q++) {
+      const uint32_t x = e + q * 32 + lane;
+      if (x < e1) mk_or(f, mk_load<W>(cur, __ldg(&a.in_src[x])));
+    }
+#pragma unroll
+    for (int q = 0; q < W; q++) acc.v[q] |= warp_or64(f.v[q]);
+    if (mk_covers(acc, need)) break;
+  }
+  unsigned long long y = 0;  // lane q ORs word q
+#pragma unroll
+  for (int q = 0; q < W; q++)
+    if (lane == q) y = acc.v[q] & need.v[q];
+  if (y) atomicOr(&a.hacc[(uint64_t)h * W + lane], y);
 }
 
 template <int W>
@@ -248,6 +325,8 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
         grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
         if (*(volatile int*)a.err) return;
       }
+      if (!push)
+        for (uint64_t c = gwarp; c < a.n_chunks; c += nwarps) ms_hub_chunk<W>(a, cur, active, c, lane);
       for (uint64_t c0 = gwarp * 32; c0 < n; c0 += nwarps * 32) {
         const uint64_t w = c0 + lane;
         Msk<W> vis = mk_zero<W>(), nw = mk_zero<W>();
@@ -271,6 +350,10 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
             if (mk_any(need)) {
               e0 = __ldg(&a.in_off[w]);
               e1 = __ldg(&a.in_off[w + 1]);
+              if (e1 - e0 > kMsHub) {  // a hub: settled from its chunks below
+                need = mk_zero<W>();
+                e1 = e0;
+              }
             }
           }
           const bool heavy = e1 - e0 > 32;
@@ -310,29 +393,26 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
 #pragma unroll
           for (int q = 0; q < W; q++) nw.v[q] = acc.v[q] & need.v[q];
         }
-        unsigned long long od = 0;
-        const bool got = mk_any(nw);
-        if (w < n) {
-          if (got) {
-            Msk<W> nv = vis;
-            mk_or(nv, nw);
-            mk_store<W>(a.visited, w, nv);
-            od = __ldg(&a.out_off[w + 1]) - __ldg(&a.out_off[w]);
-          }
-          mk_store<W>(nxt, w, nw);
-        }
-        if (__any_sync(0xffffffffu, got)) {
-#pragma unroll
-          for (int q = 0; q < W; q++) {
-            if (!__any_sync(0xffffffffu, nw.v[q] != 0)) continue;
-#pragma unroll 8
-            for (int b = 0; b < 64; b++) {
-              const unsigned c = __popc(__ballot_sync(0xffffffffu, (nw.v[q] >> b) & 1ull));
-              if (lane == 0 && c) atomicAdd(&sc[64 * q + b], c);
+        ms_settle<W>(a, nxt, w, w < n, vis, nw, sc, &s_mf, lane);
+      }
+      if (!push && a.n_hubs) {
+        // hubs: their chunks' ORs are all in hacc after the barrier
+        grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
+        if (*(volatile int*)a.err) return;
+        for (uint64_t i0 = gwarp * 32; i0 < a.n_hubs; i0 += nwarps * 32) {
+          const uint64_t i = i0 + lane;
+          uint32_t w = 0;
+          Msk<W> vis = mk_zero<W>(), nw = mk_zero<W>();
+          if (i < a.n_hubs) {
+            w = __ldg(&a.hubs[i]);
+            const Msk<W> p = mk_load<W>(a.hacc, i);
+            if (mk_any(p)) {
+              mk_store<W>(a.hacc, i, mk_zero<W>());
+              vis = mk_load<W>(a.visited, w);
+              nw = mk_andnot(p, vis);
             }
           }
-          for (int o = 16; o; o >>= 1) od += __shfl_down_sync(0xffffffffu, od, o);
-          if (lane == 0) atomicAdd(&s_mf, od);
+          ms_settle<W>(a, nxt, w, i < a.n_hubs, vis, nw, sc, &s_mf, lane);
         }
       }
       __syncthreads();
@@ -577,6 +657,40 @@ __global__ void ms_closeness_k(const unsigned long long* __restrict__ reach,
 
 }  // namespace
 
+// Builds (once per topology) the hub list and the chunks of the hubs'
+// in-edges: hubs have in-degree > kMsHub, chunks are kMsChunk slots.
+static void ensure_ms_hubs(TopoImpl* t, cudaStream_t s) {
+  ensure_in(t, s);
+  std::lock_guard<std::mutex> g(t->mu);
+  if (t->has_ms_hubs) return;
+  const uint64_t n = t->n;
+  std::vector<uint32_t> off(n + 1), hubs, chunk_hub, chunk_lo;
+  UG_CUDA(cudaMemcpyAsync(off.data(), t->in.off.get(), (n + 1) * 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  for (uint64_t w = 0; w < n; w++) {
+    if (off[w + 1] - off[w] <= kMsHub) continue;
+    for (uint32_t e = off[w]; e < off[w + 1]; e += kMsChunk) {
+      chunk_hub.push_back((uint32_t)hubs.size());
+      chunk_lo.push_back(e);
+    }
+    hubs.push_back((uint32_t)w);
+  }
+  t->ms_n_hubs = hubs.size();
+  t->ms_n_chunks = chunk_hub.size();
+  t->ms_hubs.alloc(hubs.size() ? hubs.size() : 1, s);
+  t->ms_chunk_hub.alloc(chunk_hub.size() ? chunk_hub.size() : 1, s);
+  t->ms_chunk_lo.alloc(chunk_lo.size() ? chunk_lo.size() : 1, s);
+  if (!hubs.empty()) {
+    UG_CUDA(cudaMemcpyAsync(t->ms_hubs.get(), hubs.data(), hubs.size() * 4, cudaMemcpyHostToDevice, s));
+    UG_CUDA(cudaMemcpyAsync(t->ms_chunk_hub.get(), chunk_hub.data(), chunk_hub.size() * 4,
+                            cudaMemcpyHostToDevice, s));
+    UG_CUDA(cudaMemcpyAsync(t->ms_chunk_lo.get(), chunk_lo.data(), chunk_lo.size() * 4,
+                            cudaMemcpyHostToDevice, s));
+  }
+  UG_CUDA(cudaStreamSynchronize(s));
+  t->has_ms_hubs = true;
+}
+
 // Enqueues the per-source BFS folds (reach = nodes at distance >= 1, dsum =
 // their summed distances, maxd = eccentricity) for the device ids d_src
 // (< n), following out-edges, into device arrays of n_sources entries.
@@ -595,6 +709,10 @@ static void msbfs_enqueue(TopoImpl* t, const uint32_t* d_src, uint64_t n_sources
   Scratch<unsigned long long> visited(n * W, s), fa(n * W, s), fb(n * W, s), acc(n * W, s);
   Scratch<unsigned long long> count(3 * (64 * W + 8), s);
   UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * W * 8, s));
+  ensure_ms_hubs(t, s);
+  const uint64_t nh = t->ms_n_hubs, nc = t->ms_n_chunks;
+  Scratch<unsigned long long> hacc((nh ? nh : 1) * W, s);
+  UG_CUDA(cudaMemsetAsync(hacc.get(), 0, (nh ? nh : 1) * W * 8, s));
   MsArgs a;
   a.in_off = t->in.off.get();
   a.in_src = t->in.tgt.get();
@@ -608,6 +726,12 @@ static void msbfs_enqueue(TopoImpl* t, const uint32_t* d_src, uint64_t n_sources
   a.fr0 = fa.get();
   a.fr1 = fb.get();
   a.acc = acc.get();
+  a.hubs = t->ms_hubs.get();
+  a.n_hubs = nh;
+  a.chunk_hub = t->ms_chunk_hub.get();
+  a.chunk_lo = t->ms_chunk_lo.get();
+  a.n_chunks = nc;
+  a.hacc = hacc.get();
   a.count = count.get();
   a.reach = d_reach;
   a.dsum = d_dsum;

@@ -36,6 +36,11 @@ struct TopoImpl {
   bool has_und = false;
   DevArray<uint32_t> outdeg;  // out-degree per node (PageRank shares)
   bool has_outdeg = false;
+  // Multi-source BFS: nodes whose in-edge scan is split into chunks (hubs,
+  // ascending) and each chunk's hub index and first in-CSR slot.
+  DevArray<uint32_t> ms_hubs, ms_chunk_hub, ms_chunk_lo;
+  uint64_t ms_n_hubs = 0, ms_n_chunks = 0;
+  bool has_ms_hubs = false;
   PrPlan* pr_plan = nullptr;
   std::mutex mu;
   ~TopoImpl() {
