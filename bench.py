@@ -53,6 +53,11 @@ factor 16, seed 2); GTEPS = n sources x m edges / time.
 
 --workload result: query_batch (id, degree, pagerank) on R-MAT-22 under
 Int64 user ids to a pyarrow RecordBatch, beside the per-column plain path.
+
+--workload suite: the per-kernel table (CSR build, transpose, degree,
+pagerank, BFS, weak components, triangles, clustering, weighted paths,
+betweenness) on C1 = R-MAT-16, C2 = R-MAT-22 and C3 = Poisson(16) n = 2^20
+weighted, each beside the oracle on the host cores.
 """
 
 from __future__ import annotations
@@ -633,6 +638,253 @@ def run_result(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+SUITE = ("C1", "C2", "C3")
+
+
+def run_suite(args, rank, world):
+    """Per-kernel table of the hot-path scope on the single-graph
+    configurations: C1 = R-MAT-16 (seed 1), C2 = R-MAT-22 (seed 2), C3 =
+    n = 2^20 with Poisson(16) out-degrees, uniform targets, multi-edges and
+    self-loops kept (seed 3), f32 weights U[1,10) widened to f64.  One JSON
+    line per (config, kernel): the B200 device time (events on the library's
+    launch stream around the C-ABI call, the n-sized result copied into
+    pinned host memory inside it; median over --steps after one warm call),
+    its rate, the oracle on all host cores and on one (bounded samples where
+    the full run would take minutes), and the error vs the oracle."""
+    if rank != 0:
+        return
+    import torch
+
+    torch.cuda.set_device(0)
+    from oracle import oracle as O
+    from ursa_b200 import PageRankParams, PageRankStats, Topology, _lib, gen
+
+    O.build()
+    L = _lib.load()
+    _lib.check(L.ursa_gpu_set_device(0))
+    sp = C.c_void_p()
+    _lib.check(L.ursa_gpu_thread_stream(0, C.byref(sp)))
+    lib_stream = torch.cuda.ExternalStream(sp.value)
+    cores = os.cpu_count() or 1
+    peak, peak_kind = load_peaks()
+    reps = max(args.steps, 1)
+    only = set(args.suite.split(",")) if args.suite else set(SUITE)
+
+    def pinned(n, dtype):
+        return torch.empty(max(n, 1), dtype=dtype).pin_memory().numpy()[:n]
+
+    def gpu(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(lib_stream)
+            fn()
+            e1.record(lib_stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    def cpu(fn, threads):
+        O.set_threads(threads)
+        t0 = time.perf_counter()
+        out = fn()
+        return 1e3 * (time.perf_counter() - t0), out
+
+    def emit(cfg, kernel, gpu_ms, rate, unit, cpu_ms=None, cpu_rate=None, cpu1_rate=None, error=None,
+             alg_bytes=None, **extra):
+        line = {"suite": cfg, "kernel": kernel, "gpu_ms": gpu_ms, "gpu_rate": rate, "rate_unit": unit,
+                "cpu_ms": cpu_ms, "cpu_rate": cpu_rate, "cpu_cores": cores, "cpu1_rate": cpu1_rate,
+                "speedup_vs_cpu": (rate / cpu_rate) if (rate and cpu_rate) else None, "error": error}
+        if alg_bytes:
+            gbs = alg_bytes / (gpu_ms * 1e-3) / 1e9
+            line["roofline"] = {"bound": "hbm", "achieved_gbs": gbs, "peak_gbs": peak, "peak_kind": peak_kind,
+                                "frac": gbs / peak, "frac_of_8tbs": gbs / 8000.0, "algorithmic_bytes": alg_bytes}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+
+    def rel_err(got, ref):
+        got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+        den = np.maximum(np.abs(ref), 1e-300)
+        return {"l1": float(np.abs(got - ref).sum()), "max_rel": float((np.abs(got - ref) / den).max()) if ref.size else 0.0}
+
+    def canon(labels):  # each node's label -> the smallest node id carrying it
+        _, first, inv = np.unique(np.asarray(labels, np.int64), return_index=True, return_inverse=True)
+        return first[inv]
+
+    def graph(cfg):
+        if cfg == "C1":
+            n, s, d = gen.rmat(16, 16, 1)
+            return n, s, d, None
+        if cfg == "C2":
+            n, s, d = gen.rmat(22, 16, 2)
+            return n, s, d, None
+        n, s, d = gen.poisson(1 << 20, 16.0, 3)
+        w = pinned(s.size, torch.float64)  # weights cross to the device every call: keep them pinned
+        w[:] = gen.weights_f32(s.size, 1.0, 10.0, 3)
+        return n, s, d, w
+
+    for cfg in [c for c in SUITE if c in only]:
+        n, s, d, w = graph(cfg)
+        m = int(s.size)
+        # ---- CSR build and transpose (device arrays in; Topology::build + incoming)
+        d_s = torch.from_numpy(s).cuda()
+        d_d = torch.from_numpy(d).cuda()
+        handles = []
+
+        def build_dev():
+            h = C.c_void_p()
+            _lib.check(L.ursa_gpu_topo_build_device(n, d_s.data_ptr(), d_d.data_ptr(), m, C.c_void_p(sp.value),
+                                                    C.byref(h)))
+            handles.append(h)
+
+        t_build = gpu(build_dev)
+        for hh in handles:
+            L.ursa_gpu_topo_free(hh)
+        del d_s, d_d
+        g = Topology.build(n, s, d)
+        cb_ms, ot = cpu(lambda: O.Topology(n, s, d), cores)
+        ct_ms, _ = cpu(lambda: ot.csr("in"), cores)
+        go, oo = g.out(), ot.csr("out")
+        gi, oi = g.incoming(), ot.csr("in")
+        same = all(np.array_equal(a, b) for a, b in [(go.offsets, oo[0]), (go.targets, oo[1]), (go.edge_ids, oo[2]),
+                                                     (gi.offsets, oi[0]), (gi.targets, oi[1]), (gi.edge_ids, oi[2])])
+        emit(cfg, "csr_build_and_transpose", t_build, m / (t_build * 1e-3), "edges/s", cb_ms + ct_ms,
+             m / ((cb_ms + ct_ms) * 1e-3), None, {"byte_identical": bool(same)}, 2 * (20 * m + 8 * (n + 1)),
+             input="device src/dst arrays",
+             note="the device build sorts the rows by source and by destination in one call (the endpoint "
+                  "columns are already in row order on the device); the oracle builds, then transposes",
+             cpu_build_ms=cb_ms, cpu_transpose_ms=ct_ms)
+        h = g.handle
+        deg_out = pinned(n, torch.int32)
+
+        # ---- degree
+        for dname, dval in (("out", 0), ("in", 1)):
+            t = gpu(lambda: _lib.check(L.ursa_gpu_degree(h, dval, deg_out.ctypes.data)))
+            c_ms, ref = cpu(lambda: O.degree(ot, dname), cores)
+            emit(cfg, f"degree_{dname}", t, n / (t * 1e-3), "nodes/s", c_ms, n / (c_ms * 1e-3), None,
+                 {"exact": bool(np.array_equal(deg_out.view(np.uint32), ref))}, 4 * (n + 1) + 4 * n)
+        outdeg = O.degree(ot, "out")
+
+        # ---- pagerank (plain; weighted on C3)
+        for weighted in ((False, True) if w is not None else (False,)):
+            pr = pinned(n, torch.float64)
+            stt = PageRankStats()
+            par = PageRankParams(DAMPING, MAX_ITER, TOL)
+            if weighted:
+                fn = lambda: _lib.check(L.ursa_gpu_pagerank_weighted(h, w.ctypes.data, m, C.byref(par),
+                                                                     pr.ctypes.data, C.byref(stt)))
+            else:
+                fn = lambda: _lib.check(L.ursa_gpu_pagerank(h, C.byref(par), pr.ctypes.data, C.byref(stt)))
+            t = gpu(fn)
+            iters = stt.iterations
+            if weighted:
+                c_ms, (ref, oit) = cpu(lambda: O.pagerank_weighted(ot, w, DAMPING, MAX_ITER, TOL, True), cores)
+                c1_ms, _ = cpu(lambda: O.pagerank_weighted(ot, w, DAMPING, 1, 0.0), 1)
+            else:
+                c_ms, (ref, oit) = cpu(lambda: O.pagerank(ot, DAMPING, MAX_ITER, TOL, True), cores)
+                c1_ms, _ = cpu(lambda: O.pagerank(ot, DAMPING, 1, 0.0), 1)
+            err = rel_err(pr, ref)
+            err.update({"iterations": iters, "oracle_iterations": int(oit)})
+            alg = algorithmic_bytes(n, m, iters) + (4 * m * iters if weighted else 0)
+            emit(cfg, "pagerank_weighted" if weighted else "pagerank", t, m * iters / (t * 1e-3) / 1e9, "GTEPS",
+                 c_ms, m * oit / (c_ms * 1e-3) / 1e9, m / (c1_ms * 1e-3) / 1e9, err, alg)
+
+        # ---- BFS from sampled sources with out-degree > 0
+        have_out = np.flatnonzero(outdeg > 0)
+        k_src = {"C1": 8, "C2": 64, "C3": 8}[cfg]
+        srcs = [int(have_out[i]) for i in O.sample_indices(have_out.size, k_src, {"C1": 1, "C2": 2, "C3": 3}[cfg])]
+        dist = [pinned(n, torch.int32) for _ in srcs]
+
+        def bfs_all():
+            for x, buf in zip(srcs, dist):
+                _lib.check(L.ursa_gpu_bfs_distances(h, x, 0, buf.ctypes.data))
+
+        t = gpu(bfs_all)
+        teps_edges = sum(int(outdeg[np.asarray(dd) >= 0].sum()) for dd in dist)
+        k_cpu = min(len(srcs), 8)
+        c_ms, refs = cpu(lambda: [O.bfs_distances(ot, x, "out") for x in srcs[:k_cpu]], cores)
+        exact = all(np.array_equal(dist[i], refs[i]) for i in range(k_cpu))
+        cpu_edges = sum(int(outdeg[r >= 0].sum()) for r in refs)
+        touched = teps_edges / max(len(srcs), 1)
+        emit(cfg, f"bfs_x{len(srcs)}", t, teps_edges / (t * 1e-3) / 1e9, "GTEPS", c_ms, cpu_edges / (c_ms * 1e-3) / 1e9,
+             cpu_edges / (c_ms * 1e-3) / 1e9, {"exact": bool(exact), "sources_checked": k_cpu},
+             int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
+             cpu_note="the oracle's BFS is one serial walk per source (as bfs.rs)")
+
+        # ---- weak components
+        cc = pinned(n, torch.int32)
+        t = gpu(lambda: _lib.check(L.ursa_gpu_connected_components_weak(h, cc.ctypes.data)))
+        c_ms, ref = cpu(lambda: O.connected_components_weak(ot), cores)
+        exact = bool(np.array_equal(canon(cc.view(np.uint32)), canon(ref)))
+        emit(cfg, "connected_components_weak", t, m / (t * 1e-3), "edges/s", c_ms, m / (c_ms * 1e-3),
+             m / (c_ms * 1e-3), {"same_partition": exact}, 4 * m + 4 * (n + 1) + 16 * n,
+             cpu_note="union-find is serial in the reference")
+
+        # ---- triangles and clustering (C1, C2)
+        if cfg in ("C1", "C2"):
+            ms_len = C.c_uint64()
+            _lib.check(L.ursa_gpu_topo_undirected_len(h, C.byref(ms_len)))
+            m_s = int(ms_len.value)
+            tri = pinned(n, torch.int32)
+            t = gpu(lambda: _lib.check(L.ursa_gpu_triangle_count(h, tri.ctypes.data)))
+            clu = pinned(n, torch.float64)
+            tc_ = gpu(lambda: _lib.check(L.ursa_gpu_clustering_coefficient(h, clu.ctypes.data)))
+            triangles = int(tri.view(np.uint32).astype(np.int64).sum()) // 3
+            if cfg == "C1":
+                c_ms, ref = cpu(lambda: O.triangle_count(ot), cores)
+                cc_ms, cref = cpu(lambda: O.clustering_coefficient(ot), cores)
+                e_t = {"exact": bool(np.array_equal(tri.view(np.uint32), ref))}
+                e_c = {"bit_exact": bool(np.array_equal(clu.view(np.uint64), cref.view(np.uint64)))}
+            else:
+                c_ms = cc_ms = None
+                e_t = e_c = {"checked": False,
+                             "note": "the reference's merge counting is O(sum of squared degrees) on the host "
+                                     "(hours at this scale); exact at C1 and in the GPU tests"}
+            emit(cfg, "triangle_count", t, m_s / (t * 1e-3), "undirected entries/s", c_ms,
+                 (m_s / (c_ms * 1e-3)) if c_ms else None, None, e_t, 4 * m_s + 8 * (n + 1),
+                 triangles=triangles, triangles_per_s=triangles / (t * 1e-3))
+            emit(cfg, "clustering_coefficient", tc_, m_s / (tc_ * 1e-3), "undirected entries/s", cc_ms,
+                 (m_s / (cc_ms * 1e-3)) if cc_ms else None, None, e_c, 4 * m_s + 8 * (n + 1) + 16 * n)
+
+        # ---- weighted shortest paths and betweenness (C3)
+        if cfg == "C3":
+            dd = pinned(n, torch.float64)
+            s0 = srcs[0]
+            t = gpu(lambda: _lib.check(L.ursa_gpu_dijkstra_distances(h, w.ctypes.data, m, s0, 0, dd.ctypes.data)))
+            c_ms, ref = cpu(lambda: O.dijkstra_distances(ot, w, s0, "out"), 1)
+            emit(cfg, "dijkstra_distances", t, m / (t * 1e-3) / 1e9, "GTEPS", c_ms, m / (c_ms * 1e-3) / 1e9,
+                 m / (c_ms * 1e-3) / 1e9, {"bit_exact": bool(np.array_equal(dd.view(np.uint64), ref.view(np.uint64)))},
+                 None, cpu_note="Dijkstra is serial per source")
+            fin = np.flatnonzero(np.isfinite(ref))
+            tgt = int(fin[np.argmax(ref[fin])])
+            path = pinned(n, torch.int32)
+            costs = pinned(n, torch.float64)
+            ln = C.c_int64()
+            t = gpu(lambda: _lib.check(L.ursa_gpu_shortest_path_weighted_with_cost(
+                h, w.ctypes.data, m, s0, tgt, 0, path.ctypes.data, costs.ctypes.data, n, C.byref(ln))))
+            c_ms, oref = cpu(lambda: O.shortest_path_weighted_with_cost(ot, w, s0, tgt, "out"), 1)
+            k = int(ln.value)
+            ok = oref is not None and k == len(oref[0]) and bool(np.array_equal(costs[:k], np.asarray(oref[1])))
+            emit(cfg, "shortest_path_weighted_with_cost", t, None, None, c_ms, None, None,
+                 {"cost_exact": ok, "path_len": k})
+            frac = 2.0 ** -12  # 256 sources at n = 2^20
+            for weighted in (False, True):
+                bc = pinned(n, torch.float64)
+                if weighted:
+                    fn = lambda: _lib.check(L.ursa_gpu_betweenness_weighted(h, w.ctypes.data, m, 1, frac, 1, 3,
+                                                                            bc.ctypes.data))
+                    c_ms, ref = cpu(lambda: O.betweenness_weighted(ot, w, frac, 3), cores)
+                else:
+                    fn = lambda: _lib.check(L.ursa_gpu_betweenness(h, 1, frac, 1, 3, bc.ctypes.data))
+                    c_ms, ref = cpu(lambda: O.betweenness(ot, frac, 3), cores)
+                t = gpu(fn)
+                k = 256
+                emit(cfg, "betweenness_weighted" if weighted else "betweenness", t, k * m / (t * 1e-3) / 1e9, "GTEPS",
+                     c_ms, k * m / (c_ms * 1e-3) / 1e9, None, rel_err(bc, ref), None, sources=k)
+        del g, ot
+
+
 SERVE_WORKLOAD = "serve_rmat24_uploads"
 SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
 
@@ -1026,7 +1278,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap", "closeness", "result"])
+    ap.add_argument("--workload", default="rmat22_pagerank", choices=["rmat22_pagerank", "batch", "serve", "idmap", "closeness", "result", "suite"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids (defaults give the benchmark above)
     ap.add_argument("--max-iter", type=int, default=MAX_ITER, help="pagerank max_iter (rmat22 workload)")
@@ -1035,6 +1287,7 @@ def main():
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT, help="graphs in the batch workload")
     ap.add_argument("--no-tune", action="store_true", help="batch workload: keep the default launch shapes")
     ap.add_argument("--no-plain", action="store_true", help="batch workload: skip the per-graph plain loop")
+    ap.add_argument("--suite", default="", help="suite workload: comma-separated configs (C1,C2,C3)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -1062,6 +1315,9 @@ def main():
         return
     if args.workload == "result":
         run_result(args, rank, world)
+        return
+    if args.workload == "suite":
+        run_suite(args, rank, world)
         return
 
     import torch

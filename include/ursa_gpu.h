@@ -59,6 +59,10 @@ int ursa_gpu_version(void);
 uint64_t ursa_gpu_launch_count(void);
 /* Selects the CUDA device used by topologies built afterwards on this thread. */
 int ursa_gpu_set_device(int device);
+/* The CUDA stream (a cudaStream_t) on which this host thread's calls on
+ * `device` enqueue their work: events recorded on it around a call give the
+ * call's device time. */
+int ursa_gpu_thread_stream(int device, void **stream);
 
 /* ---- Topology (ursa-core/src/topology.rs) ------------------------------ */
 

@@ -120,6 +120,7 @@ SIGNATURES = {
     "ursa_gpu_version": (i32, []),
     "ursa_gpu_launch_count": (u64, []),
     "ursa_gpu_set_device": (i32, [i32]),
+    "ursa_gpu_thread_stream": (i32, [i32, P]),
     "ursa_gpu_topo_build": (i32, [u64, P, P, u64, C.POINTER(P)]),
     "ursa_gpu_topo_build_device": (i32, [u64, P, P, u64, P, C.POINTER(P)]),
     "ursa_gpu_topo_free": (None, [P]),

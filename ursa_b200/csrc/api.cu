@@ -157,6 +157,13 @@ int ursa_gpu_set_device(int device) {
   });
 }
 
+int ursa_gpu_thread_stream(int device, void** stream) {
+  return guard([&] {
+    require(stream, "stream");
+    *stream = (void*)thread_stream(device);
+  });
+}
+
 int ursa_gpu_topo_build(uint64_t n_nodes, const uint32_t* src, const uint32_t* dst,
                         uint64_t n_edges, ursa_gpu_topo** out) {
   return guard([&] {
