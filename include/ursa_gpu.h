@@ -141,6 +141,13 @@ int ursa_gpu_pagerank_weighted(ursa_gpu_topo *t, const double *weights, uint64_t
  * -1 = unreachable; out-of-range source gives all -1.  Direction-optimising
  * (top-down / bottom-up) on the device; levels are exact. */
 int ursa_gpu_bfs_distances(ursa_gpu_topo *t, uint32_t source, int dir, int32_t *out);
+/* Extension for analytics callers: bfs_distances from each of n_sources
+ * sources at once, one bit-parallel traversal per 64 (or 256) of them;
+ * out: n_sources rows of n i32, row i = bfs_distances(sources[i], dir).
+ * Pays off with many sources; a single source is faster through
+ * ursa_gpu_bfs_distances (its frontier queues skip the untouched nodes). */
+int ursa_gpu_bfs_distances_multi(ursa_gpu_topo *t, const uint32_t *sources, uint64_t n_sources, int dir,
+                                 int32_t *out);
 
 /* shortest_path(&Topology, u32, u32, Direction) -> Option<Vec<u32>> --
  * algo/bfs.rs:48-102.  Writes the inclusive node path into path[0..cap) and

@@ -7,7 +7,7 @@ sequences (first-discoverer parents)."""
 import numpy as np
 import pytest
 
-from cases import medium_cases, small_cases
+from cases import medium_cases, random_graph, small_cases
 
 pytestmark = pytest.mark.gpu
 
@@ -124,3 +124,19 @@ def test_bfs_rmat20_sources(orc):
         src = int(cand[i])
         for dirn in ("out", "both"):
             assert np.array_equal(algo.bfs_distances(g, src, dirn), orc.bfs_distances(o, src, dirn))
+
+
+@pytest.mark.parametrize("direction", DIRS)
+def test_bfs_distances_multi(orc, direction):
+    """Many sources in one traversal: each row equals the oracle's
+    bfs_distances; 300 sources fill a 256-wide batch and a partial one, and
+    an unknown source gives a row of -1."""
+    from ursa_b200 import Topology, algo
+
+    n, s, d = random_graph(1500, 6000, 17)
+    g, o = Topology.build(n, s, d), orc.Topology(n, s, d)
+    srcs = list(range(0, 1500, 5)) + [n + 3]
+    got = algo.bfs_distances_multi(g, srcs, direction)
+    assert got.shape == (len(srcs), n)
+    for i, x in enumerate(srcs):
+        assert np.array_equal(got[i], orc.bfs_distances(o, x, direction)), (direction, x)

@@ -139,6 +139,7 @@ SIGNATURES = {
         [P, P, u64, C.POINTER(PageRankParams), P, C.POINTER(PageRankStats)],
     ),
     "ursa_gpu_bfs_distances": (i32, [P, u32, i32, P]),
+    "ursa_gpu_bfs_distances_multi": (i32, [P, P, u64, i32, P]),
     "ursa_gpu_shortest_path": (i32, [P, u32, u32, i32, P, u64, C.POINTER(i64)]),
     "ursa_gpu_dijkstra_distances": (i32, [P, P, u64, u32, i32, P]),
     "ursa_gpu_shortest_path_weighted_with_cost": (

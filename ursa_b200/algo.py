@@ -80,6 +80,17 @@ def bfs_distances(topo: Topology, source: int, direction=Direction.Out) -> np.nd
     return out
 
 
+def bfs_distances_multi(topo: Topology, sources, direction=Direction.Out) -> np.ndarray:
+    """bfs_distances from many sources in one bit-parallel traversal (an
+    extension of algo/bfs.rs:18-42): row i is bfs_distances(sources[i])."""
+    src = _u32(sources)
+    out = np.empty((src.size, topo.n_nodes()), np.int32)
+    if src.size and topo.n_nodes():
+        _lib.check(_lib.load().ursa_gpu_bfs_distances_multi(topo.handle, src.ctypes.data, src.size,
+                                                            int(Direction.of(direction)), out.ctypes.data))
+    return out
+
+
 def shortest_path(topo: Topology, source: int, target: int, direction=Direction.Out):
     """shortest_path (algo/bfs.rs:48-102): list of node ids, or None."""
     L = _lib.load()

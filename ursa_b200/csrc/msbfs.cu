@@ -29,6 +29,7 @@
 // stats' f64 sums of integer distances are exact while the total stays below
 // 2^53 (checked).  A level with no new node ends the batch.
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <vector>
 
@@ -128,11 +129,14 @@ __device__ __forceinline__ unsigned long long warp_or64(unsigned long long v) {
 }
 
 struct MsArgs {
+  // pull: the CSR whose rows list the nodes that reach each node in one step
+  // (the in-CSR when following out-edges); push: the CSR of the steps taken
   const uint32_t* in_off;
   const uint32_t* in_src;
   const uint32_t* out_off;
   const uint32_t* out_tgt;
-  uint64_t n, m;
+  uint64_t n, m;  // m: rows of the push CSR
+  int32_t* dist;  // optional: n_sources rows of n hop distances (-1 preset)
   const uint32_t* sources;  // n_sources ids < n
   uint64_t n_sources;
   uint64_t b_begin, b_end;  // batches of 64 W sources run by this launch
@@ -203,7 +207,7 @@ __device__ __forceinline__ void ms_push(const MsArgs& a, const unsigned long lon
 template <int W>
 __device__ __forceinline__ void ms_settle(const MsArgs& a, unsigned long long* nxt, uint64_t w, bool valid,
                                           const Msk<W>& vis, const Msk<W>& nw, unsigned* sc,
-                                          unsigned long long* s_mf, int lane) {
+                                          unsigned long long* s_mf, int lane, uint32_t level, uint64_t s0) {
   unsigned long long od = 0;
   const bool got = mk_any(nw);
   if (valid) {
@@ -212,6 +216,12 @@ __device__ __forceinline__ void ms_settle(const MsArgs& a, unsigned long long* n
       mk_or(nv, nw);
       mk_store<W>(a.visited, w, nv);
       od = __ldg(&a.out_off[w + 1]) - __ldg(&a.out_off[w]);
+      if (a.dist) {
+#pragma unroll
+        for (int q = 0; q < W; q++)
+          for (unsigned long long x = nw.v[q]; x; x &= x - 1)
+            a.dist[(s0 + 64 * q + (__ffsll((long long)x) - 1)) * a.n + w] = (int32_t)level;
+      }
     }
     mk_store<W>(nxt, w, nw);
   }
@@ -302,6 +312,7 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
         atomicOr(&a.visited[wd], 1ull << (threadIdx.x & 63));
         atomicOr(&a.fr0[wd], 1ull << (threadIdx.x & 63));
         atomicAdd(&a.count[S], (unsigned long long)(a.out_off[src + 1] - a.out_off[src]));
+        if (a.dist) a.dist[(s0 + threadIdx.x) * n + src] = 0;
       }
     }
     grid_barrier(a.bar, a.bar + 1, gridDim.x, a.err, kMsWaitNs);
@@ -393,7 +404,7 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
 #pragma unroll
           for (int q = 0; q < W; q++) nw.v[q] = acc.v[q] & need.v[q];
         }
-        ms_settle<W>(a, nxt, w, w < n, vis, nw, sc, &s_mf, lane);
+        ms_settle<W>(a, nxt, w, w < n, vis, nw, sc, &s_mf, lane, level, s0);
       }
       if (!push && a.n_hubs) {
         // hubs: their chunks' ORs are all in hacc after the barrier
@@ -412,7 +423,7 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
               nw = mk_andnot(p, vis);
             }
           }
-          ms_settle<W>(a, nxt, w, i < a.n_hubs, vis, nw, sc, &s_mf, lane);
+          ms_settle<W>(a, nxt, w, i < a.n_hubs, vis, nw, sc, &s_mf, lane, level, s0);
         }
       }
       __syncthreads();
@@ -437,7 +448,7 @@ __global__ void __launch_bounds__(kMsBlock) ms_persist_k(MsArgs a) {
         active.v[q] = ((unsigned long long)s_act[2 * q + 1] << 32) | s_act[2 * q];
       if (!mk_any(active)) break;
     }
-    if (blockIdx.x == 0 && threadIdx.x < k) {
+    if (blockIdx.x == 0 && threadIdx.x < k && a.reach) {
       a.reach[s0 + threadIdx.x] = reach;
       a.dsum[s0 + threadIdx.x] = dsum;
       a.maxd[s0 + threadIdx.x] = maxd;
@@ -657,15 +668,32 @@ __global__ void ms_closeness_k(const unsigned long long* __restrict__ reach,
 
 }  // namespace
 
-// Builds (once per topology) the hub list and the chunks of the hubs'
-// in-edges: hubs have in-degree > kMsHub, chunks are kMsChunk slots.
-static void ensure_ms_hubs(TopoImpl* t, cudaStream_t s) {
+// The pull and push CSRs of a traversal following `dir` (0 out-edges, 1
+// in-edges, 2 both; both uses the undirected CSR for either role).
+struct MsCsrs {
+  const uint32_t *pull_off, *pull_src, *push_off, *push_tgt;
+  uint64_t push_rows;
+};
+static MsCsrs ms_csrs(TopoImpl* t, int dir, cudaStream_t s) {
+  if (dir == 2) {
+    ensure_undirected(t, s);
+    return {t->und_off.get(), t->und_tgt.get(), t->und_off.get(), t->und_tgt.get(), t->m_und};
+  }
   ensure_in(t, s);
+  if (dir == 1) return {t->out.off.get(), t->out.tgt.get(), t->in.off.get(), t->in.tgt.get(), t->m};
+  return {t->in.off.get(), t->in.tgt.get(), t->out.off.get(), t->out.tgt.get(), t->m};
+}
+
+// Builds (once per topology and direction) the hub list and the chunks of
+// the hubs' pull rows: hubs have more than kMsHub pull entries, chunks are
+// kMsChunk slots.
+static const TopoImpl::MsHubs& ensure_ms_hubs(TopoImpl* t, int dir, const MsCsrs& c, cudaStream_t s) {
   std::lock_guard<std::mutex> g(t->mu);
-  if (t->has_ms_hubs) return;
+  TopoImpl::MsHubs& h = t->ms_hubs[dir];
+  if (h.built) return h;
   const uint64_t n = t->n;
   std::vector<uint32_t> off(n + 1), hubs, chunk_hub, chunk_lo;
-  UG_CUDA(cudaMemcpyAsync(off.data(), t->in.off.get(), (n + 1) * 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaMemcpyAsync(off.data(), c.pull_off, (n + 1) * 4, cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaStreamSynchronize(s));
   for (uint64_t w = 0; w < n; w++) {
     if (off[w + 1] - off[w] <= kMsHub) continue;
@@ -675,61 +703,65 @@ static void ensure_ms_hubs(TopoImpl* t, cudaStream_t s) {
     }
     hubs.push_back((uint32_t)w);
   }
-  t->ms_n_hubs = hubs.size();
-  t->ms_n_chunks = chunk_hub.size();
-  t->ms_hubs.alloc(hubs.size() ? hubs.size() : 1, s);
-  t->ms_chunk_hub.alloc(chunk_hub.size() ? chunk_hub.size() : 1, s);
-  t->ms_chunk_lo.alloc(chunk_lo.size() ? chunk_lo.size() : 1, s);
+  h.n_hubs = hubs.size();
+  h.n_chunks = chunk_hub.size();
+  h.hubs.alloc(hubs.size() ? hubs.size() : 1, s);
+  h.chunk_hub.alloc(chunk_hub.size() ? chunk_hub.size() : 1, s);
+  h.chunk_lo.alloc(chunk_lo.size() ? chunk_lo.size() : 1, s);
   if (!hubs.empty()) {
-    UG_CUDA(cudaMemcpyAsync(t->ms_hubs.get(), hubs.data(), hubs.size() * 4, cudaMemcpyHostToDevice, s));
-    UG_CUDA(cudaMemcpyAsync(t->ms_chunk_hub.get(), chunk_hub.data(), chunk_hub.size() * 4,
+    UG_CUDA(cudaMemcpyAsync(h.hubs.get(), hubs.data(), hubs.size() * 4, cudaMemcpyHostToDevice, s));
+    UG_CUDA(cudaMemcpyAsync(h.chunk_hub.get(), chunk_hub.data(), chunk_hub.size() * 4,
                             cudaMemcpyHostToDevice, s));
-    UG_CUDA(cudaMemcpyAsync(t->ms_chunk_lo.get(), chunk_lo.data(), chunk_lo.size() * 4,
+    UG_CUDA(cudaMemcpyAsync(h.chunk_lo.get(), chunk_lo.data(), chunk_lo.size() * 4,
                             cudaMemcpyHostToDevice, s));
   }
   UG_CUDA(cudaStreamSynchronize(s));
-  t->has_ms_hubs = true;
+  h.built = true;
+  return h;
 }
 
-// Enqueues the per-source BFS folds (reach = nodes at distance >= 1, dsum =
-// their summed distances, maxd = eccentricity) for the device ids d_src
-// (< n), following out-edges, into device arrays of n_sources entries.
+// Enqueues a BFS from each of the device ids d_src (< n) following `dir`.
+// Per source (device arrays of n_sources entries, or NULL): reach = nodes at
+// distance >= 1, dsum = their summed distances, maxd = eccentricity; d_dist
+// (or NULL): n_sources rows of n hop distances, -1 where unreached.
 // d_ctl: 4 zeroed words (grid barrier; word 2 turns nonzero if a barrier
 // wait expired).  Batches are 256 sources wide when there are enough
 // sources to fill them and the masks of a graph of at most 2^21 nodes (64 MB
 // per mask array) stay in L2; otherwise 64 wide (fewer registers per
 // thread, more warps per SM).
-static void msbfs_enqueue(TopoImpl* t, const uint32_t* d_src, uint64_t n_sources,
+static void msbfs_enqueue(TopoImpl* t, int dir, const uint32_t* d_src, uint64_t n_sources,
                           unsigned long long* d_reach, unsigned long long* d_dsum, uint32_t* d_maxd,
-                          unsigned* d_ctl, cudaStream_t s) {
+                          int32_t* d_dist, unsigned* d_ctl, cudaStream_t s) {
   const uint64_t n = t->n;
   if (n_sources == 0) return;
-  ensure_in(t, s);
+  const MsCsrs c = ms_csrs(t, dir, s);
+  const TopoImpl::MsHubs& hb = ensure_ms_hubs(t, dir, c, s);
   const int W = n_sources >= 256 && n <= (1ull << 21) ? 4 : 1;
   Scratch<unsigned long long> visited(n * W, s), fa(n * W, s), fb(n * W, s), acc(n * W, s);
   Scratch<unsigned long long> count(3 * (64 * W + 8), s);
   UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * W * 8, s));
-  ensure_ms_hubs(t, s);
-  const uint64_t nh = t->ms_n_hubs, nc = t->ms_n_chunks;
+  const uint64_t nh = hb.n_hubs, nc = hb.n_chunks;
   Scratch<unsigned long long> hacc((nh ? nh : 1) * W, s);
   UG_CUDA(cudaMemsetAsync(hacc.get(), 0, (nh ? nh : 1) * W * 8, s));
+  if (d_dist) UG_CUDA(cudaMemsetAsync(d_dist, 0xFF, n_sources * n * 4, s));
   MsArgs a;
-  a.in_off = t->in.off.get();
-  a.in_src = t->in.tgt.get();
-  a.out_off = t->out.off.get();
-  a.out_tgt = t->out.tgt.get();
+  a.in_off = c.pull_off;
+  a.in_src = c.pull_src;
+  a.out_off = c.push_off;
+  a.out_tgt = c.push_tgt;
   a.n = n;
-  a.m = t->m;
+  a.m = c.push_rows;
+  a.dist = d_dist;
   a.sources = d_src;
   a.n_sources = n_sources;
   a.visited = visited.get();
   a.fr0 = fa.get();
   a.fr1 = fb.get();
   a.acc = acc.get();
-  a.hubs = t->ms_hubs.get();
+  a.hubs = hb.hubs.get();
   a.n_hubs = nh;
-  a.chunk_hub = t->ms_chunk_hub.get();
-  a.chunk_lo = t->ms_chunk_lo.get();
+  a.chunk_hub = hb.chunk_hub.get();
+  a.chunk_lo = hb.chunk_lo.get();
   a.n_chunks = nc;
   a.hacc = hacc.get();
   a.count = count.get();
@@ -744,6 +776,21 @@ static void msbfs_enqueue(TopoImpl* t, const uint32_t* d_src, uint64_t n_sources
     ms_launch<1>(a, n_sources, t->device, s);
 }
 
+// Hop distances from each of the device ids d_src (< n), following `dir`:
+// d_dist holds n_sources rows of n (-1 where unreached); returns after the
+// work completes.
+void msbfs_distances(TopoImpl* t, int dir, const uint32_t* d_src, uint64_t n_sources, int32_t* d_dist,
+                     cudaStream_t s) {
+  if (n_sources == 0 || t->n == 0) return;
+  Scratch<unsigned> ctl(4, s);
+  UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
+  msbfs_enqueue(t, dir, d_src, n_sources, nullptr, nullptr, nullptr, d_dist, ctl.get(), s);
+  int err = 0;
+  UG_CUDA(cudaMemcpyAsync(&err, ctl.get() + 2, 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  UG_CHECK(err == 0, URSA_GPU_ETIMEOUT, "bfs: a grid barrier wait expired");
+}
+
 // Host form of msbfs_enqueue: host sources in, host folds out.
 void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_t* reach,
                uint64_t* dsum, uint32_t* maxd, cudaStream_t s) {
@@ -753,7 +800,7 @@ void msbfs_run(TopoImpl* t, const uint32_t* sources, uint64_t n_sources, uint64_
   Scratch<unsigned> ctl(4, s);
   UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
   UG_CUDA(cudaMemcpyAsync(d_src.get(), sources, n_sources * 4, cudaMemcpyHostToDevice, s));
-  msbfs_enqueue(t, d_src.get(), n_sources, d_reach.get(), d_dsum.get(), d_maxd.get(), ctl.get(), s);
+  msbfs_enqueue(t, 0, d_src.get(), n_sources, d_reach.get(), d_dsum.get(), d_maxd.get(), nullptr, ctl.get(), s);
   int err = 0;
   UG_CUDA(cudaMemcpyAsync(&err, ctl.get() + 2, 4, cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaMemcpyAsync(reach, d_reach.get(), n_sources * 8, cudaMemcpyDeviceToHost, s));
@@ -777,7 +824,7 @@ void closeness_device(TopoImpl* t, double* d_out, cudaStream_t s, float* device_
   UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 16, s));
   ms_iota_k<<<grid_for(n), kBlock, 0, s>>>(d_src.get(), n);
   UG_LAUNCH_CHECK();
-  msbfs_enqueue(t, d_src.get(), n, d_reach.get(), d_dsum.get(), d_maxd.get(), ctl.get(), s);
+  msbfs_enqueue(t, 0, d_src.get(), n, d_reach.get(), d_dsum.get(), d_maxd.get(), nullptr, ctl.get(), s);
   ms_closeness_k<<<grid_for(n), kBlock, 0, s>>>(d_reach.get(), d_dsum.get(), n, d_out);
   UG_LAUNCH_CHECK();
   UG_CUDA(cudaEventRecord(e1, s));
@@ -909,6 +956,42 @@ int ursa_gpu_closeness_device(ursa_gpu_topo* t, double* d_out, void* stream, flo
     cudaStream_t ts = thread_stream(ti->device);  // also selects the device
     cudaStream_t s = stream ? (cudaStream_t)stream : ts;
     closeness_device(ti, d_out, s, device_ms);
+  });
+}
+
+int ursa_gpu_bfs_distances_multi(ursa_gpu_topo* t, const uint32_t* sources, uint64_t n_sources, int dir,
+                                 int32_t* out) {
+  return guard([&] {
+    UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
+    UG_CHECK(dir >= 0 && dir <= 2, URSA_GPU_EINVAL, "direction must be 0, 1 or 2");
+    TopoImpl* ti = &t->impl;
+    const uint64_t n = ti->n;
+    if (n == 0 || n_sources == 0) return;
+    UG_CHECK(sources && out, URSA_GPU_EINVAL, "sources / out is NULL");
+    // bfs.rs:21-23: an unknown source's row is all -1
+    std::vector<uint32_t> valid;
+    std::vector<uint64_t> row;
+    for (uint64_t i = 0; i < n_sources; i++) {
+      if ((uint64_t)sources[i] < n) {
+        valid.push_back(sources[i]);
+        row.push_back(i);
+      } else {
+        std::memset(out + i * n, 0xFF, n * 4);
+      }
+    }
+    if (valid.empty()) return;
+    cudaStream_t s = thread_stream(ti->device);
+    Scratch<uint32_t> d_src(valid.size(), s);
+    Scratch<int32_t> d_dist(valid.size() * n, s);
+    UG_CUDA(cudaMemcpyAsync(d_src.get(), valid.data(), valid.size() * 4, cudaMemcpyHostToDevice, s));
+    msbfs_distances(ti, dir, d_src.get(), valid.size(), d_dist.get(), s);
+    if (valid.size() == n_sources) {
+      UG_CUDA(cudaMemcpyAsync(out, d_dist.get(), n_sources * n * 4, cudaMemcpyDeviceToHost, s));
+    } else {
+      for (size_t j = 0; j < valid.size(); j++)
+        UG_CUDA(cudaMemcpyAsync(out + row[j] * n, d_dist.get() + j * n, n * 4, cudaMemcpyDeviceToHost, s));
+    }
+    UG_CUDA(cudaStreamSynchronize(s));
   });
 }
 

@@ -36,11 +36,14 @@ struct TopoImpl {
   bool has_und = false;
   DevArray<uint32_t> outdeg;  // out-degree per node (PageRank shares)
   bool has_outdeg = false;
-  // Multi-source BFS: nodes whose in-edge scan is split into chunks (hubs,
-  // ascending) and each chunk's hub index and first in-CSR slot.
-  DevArray<uint32_t> ms_hubs, ms_chunk_hub, ms_chunk_lo;
-  uint64_t ms_n_hubs = 0, ms_n_chunks = 0;
-  bool has_ms_hubs = false;
+  // Multi-source BFS, per direction (out, in, both): nodes whose pull scan
+  // is split into chunks (hubs, ascending) and each chunk's hub index and
+  // first slot of the pull CSR.
+  struct MsHubs {
+    DevArray<uint32_t> hubs, chunk_hub, chunk_lo;
+    uint64_t n_hubs = 0, n_chunks = 0;
+    bool built = false;
+  } ms_hubs[3];
   PrPlan* pr_plan = nullptr;
   std::mutex mu;
   ~TopoImpl() {
@@ -83,6 +86,8 @@ void clustering_run(TopoImpl* t, double* d_out, cudaStream_t s);
 void betweenness_run(TopoImpl* t, const double* d_weights, bool has_sample, double sample,
                      bool has_seed, uint64_t seed, double* d_out, cudaStream_t s);
 void closeness_device(TopoImpl* t, double* d_out, cudaStream_t s, float* device_ms);
+void msbfs_distances(TopoImpl* t, int dir, const uint32_t* d_src, uint64_t n_sources, int32_t* d_dist,
+                     cudaStream_t s);
 void closeness_weighted_device(TopoImpl* t, const double* d_w, double* d_out, cudaStream_t s);
 
 // k_hop pairs (seed, reached) in the reference's emission order, on the host.
