@@ -388,12 +388,13 @@ int ursa_gpu_betweenness_weighted(ursa_gpu_topo* t, const double* weights, uint6
     UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
-    check_sssp_weights(weights, ti->m);
+    UG_CHECK(ti->m == 0 || weights, URSA_GPU_EINVAL, "weights is NULL");
     if (ti->n == 0) return;  // betweenness.rs:248-250
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);
     Scratch<double> dw(ti->m ? ti->m : 1, s), d(ti->n, s);
     if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
+    check_sssp_weights_device(dw.get(), ti->m, s);
     betweenness_run(ti, dw.get(), has_sample != 0, sample, has_seed != 0, seed, d.get(), s);
     UG_CUDA(cudaMemcpyAsync(out, d.get(), ti->n * 8, cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));

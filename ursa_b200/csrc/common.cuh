@@ -46,16 +46,12 @@ void count_launch();
 
 constexpr int kBlock = 256;
 
-// Edge weights for the shortest-path family: non-null when there are edges
-// and none negative, as evaluate_weight requires before any weighted kernel
-// runs (ursa-plan/src/weight.rs:88-93).  Negative weights would also let a
-// frontier Bellman-Ford cycle forever.
-inline void check_sssp_weights(const double* w, uint64_t m) {
-  if (m == 0) return;
-  if (!w) throw Error(URSA_GPU_EINVAL, "weights is NULL");
-  for (uint64_t i = 0; i < m; i++)
-    if (w[i] < 0.0) throw Error(URSA_GPU_EINVAL, "weights must be non-negative");
-}
+// Edge weights for the shortest-path family, once on the device (d_w: m
+// f64): URSA_GPU_EINVAL if any is negative, as evaluate_weight requires
+// before any weighted kernel runs (ursa-plan/src/weight.rs:88-93; NaN
+// passes there too).  Negative weights would also let a frontier
+// Bellman-Ford cycle forever, so this runs before one starts.
+void check_sssp_weights_device(const double* d_w, uint64_t m, cudaStream_t s);
 
 inline unsigned grid_for(uint64_t n, int block = kBlock, unsigned cap = 148u * 32u) {
   uint64_t g = (n + block - 1) / block;

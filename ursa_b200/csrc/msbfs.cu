@@ -1001,13 +1001,14 @@ int ursa_gpu_closeness_weighted(ursa_gpu_topo* t, const double* weights, uint64_
     UG_CHECK(t, URSA_GPU_EINVAL, "topology is NULL");
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
-    check_sssp_weights(weights, ti->m);
+    UG_CHECK(ti->m == 0 || weights, URSA_GPU_EINVAL, "weights is NULL");
     const uint64_t n = ti->n;
     if (n == 0) return;
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);
     Scratch<double> dw(ti->m ? ti->m : 1, s), d_out(n, s);
     if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
+    check_sssp_weights_device(dw.get(), ti->m, s);
     closeness_weighted_device(ti, dw.get(), d_out.get(), s);
     UG_CUDA(cudaMemcpyAsync(out, d_out.get(), n * 8, cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));

@@ -291,4 +291,26 @@ void offsets_from_sorted(const uint32_t* sorted_keys, uint64_t m, uint64_t n, ui
   UG_LAUNCH_CHECK();
 }
 
+namespace {
+__global__ void any_negative_k(const double* __restrict__ w, uint64_t m, unsigned* __restrict__ bad) {
+  bool neg = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    neg |= __ldg(&w[i]) < 0.0;
+  if (__any_sync(0xffffffffu, neg) && (threadIdx.x & 31) == 0) *bad = 1u;
+}
+}  // namespace
+
+void check_sssp_weights_device(const double* d_w, uint64_t m, cudaStream_t s) {
+  if (m == 0) return;
+  Scratch<unsigned> bad(1, s);
+  UG_CUDA(cudaMemsetAsync(bad.get(), 0, 4, s));
+  any_negative_k<<<grid_for(m, kBlock, 148u * 16u), kBlock, 0, s>>>(d_w, m, bad.get());
+  UG_LAUNCH_CHECK();
+  unsigned h = 0;
+  UG_CUDA(cudaMemcpyAsync(&h, bad.get(), 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  UG_CHECK(h == 0, URSA_GPU_EINVAL, "weights must be non-negative");
+}
+
 }  // namespace ug

@@ -196,10 +196,8 @@ const char* column_format(const ursa_gpu_output_column& c, uint64_t m, size_t* w
       return "g";
     case URSA_GPU_ALGO_BETWEENNESS:
     case URSA_GPU_ALGO_CLOSENESS:
-      if (weighted) {
-        UG_CHECK(c.n_weights == m, URSA_GPU_EINVAL, "weights length must equal the edge count");
-        check_sssp_weights(c.weights, m);
-      }
+      UG_CHECK(!weighted || c.n_weights == m, URSA_GPU_EINVAL,
+               "weights length must equal the edge count");
       *width = 8;
       return "g";
     case URSA_GPU_ALGO_LABEL_PROPAGATION:
@@ -216,6 +214,8 @@ void compute_column(TopoImpl* t, const ursa_gpu_output_column& c, uint8_t* d_dst
   if (c.weights && t->m) {
     dw.alloc(t->m, s);
     UG_CUDA(cudaMemcpyAsync(dw.get(), c.weights, t->m * 8, cudaMemcpyHostToDevice, s));
+    if (c.algo == URSA_GPU_ALGO_BETWEENNESS || c.algo == URSA_GPU_ALGO_CLOSENESS)
+      check_sssp_weights_device(dw.get(), t->m, s);
   }
   const double* w = c.weights ? (t->m ? dw.get() : nullptr) : nullptr;
   const bool weighted = c.weights != nullptr;
@@ -371,7 +371,7 @@ int ursa_gpu_path_batch(ursa_gpu_topo* t, ursa_gpu_idmap* ids, uint32_t source, 
     check_ids(ti, ids);
     if (weights) {
       UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
-      check_sssp_weights(weights, ti->m);
+      UG_CHECK(ti->m == 0 || weights, URSA_GPU_EINVAL, "weights is NULL");
     }
     const uint64_t n = ti->n;
     cudaStream_t s = thread_stream(ti->device);
@@ -381,6 +381,7 @@ int ursa_gpu_path_batch(ursa_gpu_topo* t, ursa_gpu_idmap* ids, uint32_t source, 
     if (weights) {
       Scratch<double> dw(ti->m ? ti->m : 1, s);
       if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
+      check_sssp_weights_device(dw.get(), ti->m, s);
       len = weighted_path_run(ti, dw.get(), source, target, dir, path.data(), costs.data(), path.size(), s);
     } else {
       len = shortest_path_run(ti, source, target, dir, path.data(), path.size(), s);

@@ -341,12 +341,13 @@ int ursa_gpu_dijkstra_distances(ursa_gpu_topo* t, const double* weights, uint64_
     UG_CHECK(dir >= 0 && dir <= 2, URSA_GPU_EINVAL, "direction must be 0, 1 or 2");
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
-    check_sssp_weights(weights, ti->m);
+    UG_CHECK(ti->m == 0 || weights, URSA_GPU_EINVAL, "weights is NULL");
     if (ti->n == 0) return;
     UG_CHECK(out, URSA_GPU_EINVAL, "out is NULL");
     cudaStream_t s = thread_stream(ti->device);
     Scratch<double> dw(ti->m ? ti->m : 1, s), dout(ti->n, s);
     if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
+    check_sssp_weights_device(dw.get(), ti->m, s);
     dijkstra_run(ti, dw.get(), source, dir, dout.get(), s);
     UG_CUDA(cudaMemcpyAsync(out, dout.get(), ti->n * 8, cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));
@@ -363,10 +364,11 @@ int ursa_gpu_shortest_path_weighted_with_cost(ursa_gpu_topo* t, const double* we
     *len = -1;
     TopoImpl* ti = &t->impl;
     UG_CHECK(n_weights == ti->m, URSA_GPU_EINVAL, "weights length must equal the edge count");
-    check_sssp_weights(weights, ti->m);
+    UG_CHECK(ti->m == 0 || weights, URSA_GPU_EINVAL, "weights is NULL");
     cudaStream_t s = thread_stream(ti->device);
     Scratch<double> dw(ti->m ? ti->m : 1, s);
     if (ti->m) UG_CUDA(cudaMemcpyAsync(dw.get(), weights, ti->m * 8, cudaMemcpyHostToDevice, s));
+    check_sssp_weights_device(dw.get(), ti->m, s);
     int64_t r = weighted_path_run(ti, dw.get(), source, target, dir, path, costs, cap, s);
     if (r < -1) {
       *len = -r - 2;
