@@ -730,17 +730,19 @@ def run_suite(args, rank, world):
         # ---- CSR build and transpose (device arrays in; Topology::build + incoming)
         d_s = torch.from_numpy(s).cuda()
         d_d = torch.from_numpy(d).cuda()
-        handles = []
-
-        def build_dev():
+        tb = []
+        for r in range(reps + 1):  # each build freed before the next (outside the timed span)
             h = C.c_void_p()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(lib_stream)
             _lib.check(L.ursa_gpu_topo_build_device(n, d_s.data_ptr(), d_d.data_ptr(), m, C.c_void_p(sp.value),
                                                     C.byref(h)))
-            handles.append(h)
-
-        t_build = gpu(build_dev)
-        for hh in handles:
-            L.ursa_gpu_topo_free(hh)
+            e1.record(lib_stream)
+            e1.synchronize()
+            if r:
+                tb.append(e0.elapsed_time(e1))
+            L.ursa_gpu_topo_free(h)
+        t_build = statistics.median(tb)
         del d_s, d_d
         g = Topology.build(n, s, d)
         cb_ms, ot = cpu(lambda: O.Topology(n, s, d), cores)
