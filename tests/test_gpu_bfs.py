@@ -140,3 +140,20 @@ def test_bfs_distances_multi(orc, direction):
     assert got.shape == (len(srcs), n)
     for i, x in enumerate(srcs):
         assert np.array_equal(got[i], orc.bfs_distances(o, x, direction)), (direction, x)
+
+
+@pytest.mark.parametrize("direction", DIRS)
+def test_bfs_distances_multi_hubs(orc, direction):
+    """Hubs in every direction: node 0 has 2,499 in-edges, node 1 has 1,800
+    out-edges (split scans for out, in and both traversals)."""
+    from ursa_b200 import Topology, algo
+
+    rng = np.random.default_rng(23)
+    s = list(range(2, 2500)) + [1] * 1800 + rng.integers(2, 2600, 4000).tolist()
+    d = [0] * 2498 + list(range(700, 2500)) + rng.integers(2, 2600, 4000).tolist()
+    n = 2600
+    g, o = Topology.build(n, s, d), orc.Topology(n, s, d)
+    srcs = list(range(0, n, 7))
+    got = algo.bfs_distances_multi(g, srcs, direction)
+    for i, x in enumerate(srcs):
+        assert np.array_equal(got[i], orc.bfs_distances(o, x, direction)), (direction, x)
