@@ -23,6 +23,7 @@ struct StreamSlot {
   }
 };
 thread_local StreamSlot g_streams;
+thread_local StreamSlot g_aux_streams;  // a second stream per thread: copies that overlap work
 std::mutex g_dev_mu;
 int g_sm_count[64] = {0};
 bool g_prepared[64] = {false};
@@ -47,7 +48,7 @@ __global__ void check_range_k(const uint32_t* __restrict__ a, const uint32_t* __
                               uint64_t m, uint64_t n, unsigned* __restrict__ bad) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
        i += (uint64_t)gridDim.x * blockDim.x)
-    if ((uint64_t)a[i] >= n || (uint64_t)b[i] >= n) atomicOr(bad, 1u);
+    if ((uint64_t)a[i] >= n || (b && (uint64_t)b[i] >= n)) atomicOr(bad, 1u);
 }
 }  // namespace
 
@@ -95,6 +96,14 @@ cudaStream_t thread_stream(int device) {
   return s;
 }
 
+// The thread's second stream on `device` (overlapping host-to-device copies).
+static cudaStream_t thread_aux_stream(int device) {
+  thread_stream(device);
+  cudaStream_t& s = g_aux_streams.s[device];
+  if (!s) UG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  return s;
+}
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 static cudaStream_t call_stream(TopoImpl* t, void* stream) {
@@ -107,34 +116,42 @@ static void require(const void* p, const char* what) {
 }
 
 TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m,
-                           cudaStream_t s, int device, ursa_gpu_topo** holder) {
+                           cudaStream_t s, int device, ursa_gpu_topo** holder, cudaEvent_t dst_ready) {
   UG_CHECK(m <= 0xFFFFFFFFull, URSA_GPU_EINVAL,
            "more than u32::MAX (~4.29B) edges is beyond the edge-id cap");
   UG_CHECK(n <= 0xFFFFFFFFull, URSA_GPU_EINVAL, "more than u32::MAX nodes");
-  if (m) {
-    Scratch<unsigned> bad(1, s);
-    UG_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(unsigned), s));
-    check_range_k<<<grid_for(m), kBlock, 0, s>>>(d_src, d_dst, m, n, bad.get());
-    UG_LAUNCH_CHECK();
-    unsigned hb = 0;
-    UG_CUDA(cudaMemcpyAsync(&hb, bad.get(), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    UG_CUDA(cudaStreamSynchronize(s));
-    UG_CHECK(hb == 0, URSA_GPU_EINVAL, "dense endpoint id out of range (>= n_nodes)");
-  }
   auto* h = new ursa_gpu_topo();
   *holder = h;
   TopoImpl* t = &h->impl;
   t->device = device;
   t->n = n;
   t->m = m;
-  build_csr(n, d_src, d_dst, m, t->out, s);
+  // The endpoint range check is read once at the end: the sort masks every
+  // digit and its gathers index row positions, so out-of-range ids cannot
+  // make it touch memory out of bounds -- the result is only discarded.
+  Scratch<unsigned> bad(1, s);
+  UG_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(unsigned), s));
+  if (m) {
+    check_range_k<<<grid_for(m), kBlock, 0, s>>>(d_src, nullptr, m, n, bad.get());
+    UG_LAUNCH_CHECK();
+  }
+  // Out-CSR: rows by source; the destinations are only gathered in the last
+  // radix pass, so they may still be arriving (dst_ready) until then.
+  build_csr(n, d_src, d_dst, m, t->out, s, dst_ready);
+  if (m) {
+    check_range_k<<<grid_for(m), kBlock, 0, s>>>(d_dst, nullptr, m, n, bad.get());
+    UG_LAUNCH_CHECK();
+  }
   // The endpoint columns are on the device in row order right now, so the
   // transpose is a second stable sort by destination -- the same in-CSR the
   // lazy reconstruction would produce (topology.rs:343-348), without
   // un-permuting the out-CSR later.
   build_csr(n, d_dst, d_src, m, t->in, s);
   t->has_in = true;
+  unsigned hb = 0;
+  UG_CUDA(cudaMemcpyAsync(&hb, bad.get(), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   UG_CUDA(cudaStreamSynchronize(s));
+  UG_CHECK(hb == 0, URSA_GPU_EINVAL, "dense endpoint id out of range (>= n_nodes)");
   return t;
 }
 
@@ -177,18 +194,30 @@ int ursa_gpu_topo_build(uint64_t n_nodes, const uint32_t* src, const uint32_t* d
              "more than u32::MAX (~4.29B) edges is beyond the edge-id cap");
     int dev = g_device;
     cudaStream_t s = thread_stream(dev);
+    cudaStream_t s2 = thread_aux_stream(dev);
     Scratch<uint32_t> d_src(n_edges, s), d_dst(n_edges, s);
-    if (n_edges) {
-      UG_CUDA(cudaMemcpyAsync(d_src.get(), src, n_edges * 4, cudaMemcpyHostToDevice, s));
-      UG_CUDA(cudaMemcpyAsync(d_dst.get(), dst, n_edges * 4, cudaMemcpyHostToDevice, s));
-    }
+    // src first on this stream; dst on the second stream right behind it, so
+    // the out-CSR's radix passes over src run while dst crosses the link
+    cudaEvent_t src_in = nullptr, dst_in = nullptr;
+    UG_CUDA(cudaEventCreateWithFlags(&src_in, cudaEventDisableTiming));
+    UG_CUDA(cudaEventCreateWithFlags(&dst_in, cudaEventDisableTiming));
     ursa_gpu_topo* h = nullptr;
     try {
-      topo_from_device(n_nodes, d_src.get(), d_dst.get(), n_edges, s, dev, &h);
+      if (n_edges) UG_CUDA(cudaMemcpyAsync(d_src.get(), src, n_edges * 4, cudaMemcpyHostToDevice, s));
+      UG_CUDA(cudaEventRecord(src_in, s));
+      UG_CUDA(cudaStreamWaitEvent(s2, src_in, 0));
+      if (n_edges) UG_CUDA(cudaMemcpyAsync(d_dst.get(), dst, n_edges * 4, cudaMemcpyHostToDevice, s2));
+      UG_CUDA(cudaEventRecord(dst_in, s2));
+      topo_from_device(n_nodes, d_src.get(), d_dst.get(), n_edges, s, dev, &h, dst_in);
     } catch (...) {
+      UG_CUDA(cudaStreamWaitEvent(s, dst_in, 0));  // d_dst is freed on s
       delete h;
+      cudaEventDestroy(src_in);
+      cudaEventDestroy(dst_in);
       throw;
     }
+    cudaEventDestroy(src_in);
+    cudaEventDestroy(dst_in);
     *out = h;
   });
 }

@@ -128,10 +128,16 @@ __global__ void __launch_bounds__(kBlock) radix_upsweep_k(const uint32_t* __rest
   uint32_t tile = blockIdx.x;
   uint64_t base = (uint64_t)tile * kRadixTile;
   int w = threadIdx.x >> 5;
-#pragma unroll 4
+  uint32_t k[kRadixItems];
+#pragma unroll
   for (int i = 0; i < kRadixItems; i++) {
-    uint64_t idx = base + (uint64_t)i * kBlock + threadIdx.x;
-    if (idx < n) atomicAdd(&cnt[w][(keys[idx] >> shift) & mask], 1u);
+    const uint64_t idx = base + (uint64_t)i * kBlock + threadIdx.x;
+    k[i] = idx < n ? __ldg(&keys[idx]) : 0u;
+  }
+#pragma unroll
+  for (int i = 0; i < kRadixItems; i++) {
+    const uint64_t idx = base + (uint64_t)i * kBlock + threadIdx.x;
+    if (idx < n) atomicAdd(&cnt[w][(k[i] >> shift) & mask], 1u);
   }
   __syncthreads();
   for (int d = threadIdx.x; d < 256; d += kBlock) {
@@ -159,12 +165,19 @@ __global__ void __launch_bounds__(kBlock) radix_downsweep_k(
   // items w*512 + i*32 + lane, so (round, lane) order is input order.
   const uint64_t wbase = (uint64_t)tile * kRadixTile + (uint64_t)w * (32 * kRadixItems);
   uint32_t k[kRadixItems], v[kRadixItems], dr[kRadixItems];
+  // all of the warp's loads in flight before the first ranking step
+#pragma unroll
+  for (int i = 0; i < kRadixItems; i++) {
+    const uint64_t idx = wbase + (uint64_t)i * 32 + lane;
+    const bool valid = idx < n;
+    k[i] = valid ? __ldg(&keys_in[idx]) : 0u;
+    v[i] = valid ? (vals_in ? __ldg(&vals_in[idx]) : (uint32_t)idx) : 0u;
+  }
 #pragma unroll
   for (int i = 0; i < kRadixItems; i++) {
     uint64_t idx = wbase + (uint64_t)i * 32 + lane;
     bool valid = idx < n;
-    uint32_t key = valid ? keys_in[idx] : 0u;
-    uint32_t val = valid ? (vals_in ? vals_in[idx] : (uint32_t)idx) : 0u;
+    uint32_t key = k[i];
     uint32_t d = valid ? ((key >> shift) & mask) : 256u;
     uint32_t peers = __match_any_sync(0xffffffffu, d);
     uint32_t rank_in = __popc(peers & lt);
@@ -172,8 +185,6 @@ __global__ void __launch_bounds__(kBlock) radix_downsweep_k(
     __syncwarp();
     if (d < 256u && rank_in == 0) wcnt[w][d] = before + __popc(peers);
     __syncwarp();
-    k[i] = key;
-    v[i] = val;
     dr[i] = (d << 16) | (before + rank_in);
   }
   __syncthreads();
@@ -247,7 +258,7 @@ void exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t*
 
 void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint64_t n, int key_bits,
                       uint32_t* keys_out, uint32_t* vals_out, const uint32_t* gather_src,
-                      uint32_t* gather_out, cudaStream_t s) {
+                      uint32_t* gather_out, cudaStream_t s, cudaEvent_t gather_ready) {
   UG_CHECK(n < (1ull << 32), URSA_GPU_EINVAL, "radix sort: more than 2^32-1 items");
   if (n == 0) return;
   int passes = key_bits <= 8 ? 1 : (key_bits + 7) / 8;
@@ -276,6 +287,7 @@ void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint64_t
     radix_upsweep_k<<<num_tiles, kBlock, 0, s>>>(kin, n, shift, mask, hist.get(), num_tiles);
     UG_LAUNCH_CHECK();
     exclusive_scan_u32(hist.get(), hist.get(), (uint64_t)256 * num_tiles, nullptr, s);
+    if (last && gather_ready) UG_CUDA(cudaStreamWaitEvent(s, gather_ready, 0));
     radix_downsweep_k<<<num_tiles, kBlock, 0, s>>>(kin, vin, n, shift, mask, hist.get(), num_tiles,
                                                    kout, vout, last ? gather_src : nullptr,
                                                    gather_out);

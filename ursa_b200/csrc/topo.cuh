@@ -54,7 +54,8 @@ struct TopoImpl {
 // Stable counting-sort CSR build from device endpoint arrays (keys group,
 // other is the paired endpoint); row order is kept inside each segment.
 void build_csr(uint64_t n, const uint32_t* d_keys, const uint32_t* d_other, uint64_t m,
-               DevCsr& out, cudaStream_t s);
+               DevCsr& out, cudaStream_t s,
+               cudaEvent_t other_ready = nullptr);
 // Lazily built parts; each call is a no-op once built.
 void ensure_in(TopoImpl* t, cudaStream_t s);
 void ensure_undirected(TopoImpl* t, cudaStream_t s);
@@ -70,7 +71,8 @@ void orient_build(TopoImpl* t, OrientedCsr& o, cudaStream_t s);
 void triangle_count_oriented(const OrientedCsr& o, uint64_t n, uint32_t* d_tri, cudaStream_t s);
 void cc_weak_with_parent(TopoImpl* t, uint32_t* parent, uint32_t* d_out, cudaStream_t s);
 TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m,
-                           cudaStream_t s, int device, ursa_gpu_topo** holder);
+                           cudaStream_t s, int device, ursa_gpu_topo** holder,
+                           cudaEvent_t dst_ready = nullptr);
 
 // Slot -> owning node for a CSR (binary search over offsets), n_slots = m.
 void csr_owners(const uint32_t* off, uint64_t n, uint64_t m, uint32_t* owner, cudaStream_t s);
