@@ -94,6 +94,22 @@ def env_int(name, default):
         return default
 
 
+def combine_replicas(dist, device, t_dev_ms, t_e2e_s, edges, e2e_edges):
+    """Replicas (one independent copy of the workload per rank): the job's
+    times are the slowest rank's, its work the sum of every rank's.  dist is
+    torch.distributed (any backend) or None for one process; returns
+    (t_dev_ms, t_e2e_s, edges, e2e_edges) as floats."""
+    if dist is None:
+        return float(t_dev_ms), float(t_e2e_s), float(edges), float(e2e_edges)
+    import torch
+
+    tt = torch.tensor([float(t_dev_ms), float(t_e2e_s)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    ei = torch.tensor([float(edges), float(e2e_edges)], dtype=torch.float64, device=device)
+    dist.all_reduce(ei, op=dist.ReduceOp.SUM)
+    return float(tt[0]), float(tt[1]), float(ei[0]), float(ei[1])
+
+
 def algorithmic_bytes(n: int, m: int, iters: int) -> int:
     """Compulsory HBM bytes of one pagerank launch.
 
@@ -1415,17 +1431,8 @@ def main():
             e2e_iters.append(it)
 
     # ---- max over ranks
-    t_dev = total_ms
-    t_e2e = sum(e2e_times)
-    if dist:
-        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(tt[0]), float(tt[1])
-        ei = torch.tensor([float(edges_iters), float(m * sum(e2e_iters))], dtype=torch.float64, device="cuda")
-        dist.all_reduce(ei, op=dist.ReduceOp.SUM)
-        edges_iters_all, e2e_edges_all = float(ei[0]), float(ei[1])
-    else:
-        edges_iters_all, e2e_edges_all = float(edges_iters), float(m * sum(e2e_iters))
+    t_dev, t_e2e, edges_iters_all, e2e_edges_all = combine_replicas(
+        dist, "cuda", total_ms, sum(e2e_times), edges_iters, m * sum(e2e_iters))
 
     if rank == 0:
         iters = stats[-1].iterations
