@@ -229,7 +229,7 @@ def run_reference(args, rank, world):
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": TOL,
                    "max_iter": MAX_ITER, "iterations": iters[-1], "l2": "inputs larger than L2",
-                   "parallelism": "replicas"},
+                   "parallelism": "replicas" if world > 1 else "single"},
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "port",
                          "sample": "full Topology::build + transpose + pagerank to tol per step "
                                    "(C restatement of ursa-core; the Rust crate cannot be built here)"},
