@@ -13,10 +13,11 @@
 //   (need = active & ~visited[w]) ORs its in-neighbours' frontier masks,
 //   stopping as soon as every needed bit is found; new = acc & need.
 //   Nodes with at most 32 edges to scan are handled by one lane, up to
-//   kMsHub by the whole warp; a hub's in-edges are cut into kMsChunk-edge
-//   chunks that any warp takes, ORed into a per-hub accumulator and settled
-//   after one more barrier (one warp per hub put every other warp at the
-//   barrier waiting for it).  visited[w] |= new; next[w] = new.
+//   kMsHub by the whole warp; the in-edges of longer rows are cut into
+//   kMsChunk-edge chunks that any warp takes, ORed into a per-row
+//   accumulator and settled after one more barrier (a warp scanning long
+//   rows one after another held every other warp at the level barrier).
+//   visited[w] |= new; next[w] = new.
 // A source that reached no new node on a level is finished and leaves the
 // active mask.  Per source, the number of nodes first reached on the level is
 // a column popcount of the new masks (one warp ballot per bit), summed per
@@ -45,8 +46,8 @@ constexpr int kMsWarps = kMsBlock / 32;
 constexpr uint64_t kMsSourcesPerLaunch = 1024;
 constexpr uint64_t kMsWaitNs = 5000000000ull;  // one grid-barrier wait
 constexpr uint64_t kMsPushDiv = 8;  // push while the frontier's out-edges are below m / 8
-constexpr uint32_t kMsHub = 512;    // in-degree above which a node's scan is split
-constexpr uint32_t kMsChunk = 512;  // in-edges per chunk of a split scan
+constexpr uint32_t kMsHub = 64;    // in-degree above which a node's scan is split
+constexpr uint32_t kMsChunk = 128;  // in-edges per chunk of a split scan
 
 // W 64-bit words per node: bit j of word q belongs to source 64 q + j of the
 // batch.  A node's W words are contiguous (one 32-byte sector for W = 4).
