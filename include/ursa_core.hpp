@@ -10,7 +10,8 @@
 // k_hop, connected_components_weak, triangle_count, clustering_coefficient,
 // betweenness, betweenness_weighted, closeness and closeness_weighted
 // (algo/closeness.rs:69-224), plus ursa-plan's avg_path_length and diameter
-// (ursa-plan/src/stats.rs:142-167).  Vec<T> becomes std::vector<T>,
+// (ursa-plan/src/stats.rs:142-167) and, as an extension with no ursa-core
+// counterpart, bfs_distances_multi.  Vec<T> becomes std::vector<T>,
 // Option<T> becomes std::optional<T>.  Where the Rust code would panic (a
 // contract violation, e.g. a weights length that is not the edge count), the
 // mirror throws ursa_core::Error carrying the C ABI status and message.
@@ -126,6 +127,22 @@ inline std::vector<double> pagerank_weighted(const Topology& t, const std::vecto
 inline std::vector<int32_t> bfs_distances(const Topology& t, uint32_t source, Direction dir) {
   std::vector<int32_t> out(t.n_nodes());
   check(ursa_gpu_bfs_distances(t.handle(), source, (int)dir, out.data()));
+  return out;
+}
+
+// Extension (no ursa-core counterpart): bfs_distances from many sources in
+// one bit-parallel traversal; row i of the result is bfs_distances(sources[i]).
+inline std::vector<std::vector<int32_t>> bfs_distances_multi(const Topology& t,
+                                                             const std::vector<uint32_t>& sources,
+                                                             Direction dir) {
+  const uint64_t n = t.n_nodes();
+  std::vector<int32_t> flat(sources.size() * n);
+  if (!sources.empty() && n)
+    check(ursa_gpu_bfs_distances_multi(t.handle(), sources.data(), sources.size(), (int)dir,
+                                       flat.data()));
+  std::vector<std::vector<int32_t>> out(sources.size());
+  for (size_t i = 0; i < sources.size(); i++)
+    out[i].assign(flat.begin() + i * n, flat.begin() + (i + 1) * n);
   return out;
 }
 

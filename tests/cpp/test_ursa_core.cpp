@@ -48,6 +48,9 @@ int main() {
   EXPECT(algo::shortest_path(p, 0, 3, D::Out) == std::optional<std::vector<uint32_t>>({0, 1, 2, 3}));
   EXPECT(!algo::shortest_path(p, 3, 0, D::Out).has_value());
   EXPECT(algo::shortest_path(p, 3, 0, D::In) == std::optional<std::vector<uint32_t>>({3, 2, 1, 0}));
+  auto multi = algo::bfs_distances_multi(p, {0, 2, 9}, D::Out);  // 9: unknown source, all -1
+  EXPECT(multi.size() == 3 && multi[0] == algo::bfs_distances(p, 0, D::Out) &&
+         eq(multi[1], {-1, -1, 0, 1, -1}) && eq(multi[2], {-1, -1, -1, -1, -1}));
   // bfs.rs:366-387
   Topology w = Topology::build(4, {0, 1, 0}, {1, 3, 3});
   auto wc = algo::shortest_path_weighted_with_cost(w, {1.0, 1.0, 5.0}, 0, 3, D::Out);
