@@ -18,15 +18,24 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc_labels(g, n):
+def _noalloc_labels(g, n, stream=None):
+    """Labels through the allocation-free entry point; stream is a torch
+    stream whose handle is passed (the caller's stream), or None for the
+    library's own stream for this thread."""
     import torch
 
     from ursa_b200 import _lib
 
-    out = torch.full((max(n, 1),), 0xFFFFFFF, dtype=torch.int32, device="cuda")
+    out = torch.full((max(n, 1),), 0xFFFFFFF, dtype=torch.int32, device="cuda:0")
     torch.cuda.synchronize()
-    _lib.check(_lib.load().ursa_gpu_connected_components_weak_noalloc(g.handle, out.data_ptr(), None))
+    h = None if stream is None else stream.cuda_stream
+    _lib.check(_lib.load().ursa_gpu_connected_components_weak_noalloc(g.handle, out.data_ptr(), h))
     return out[:n].cpu().numpy().view(np.uint32)
+
+
+def _canon(labels):
+    _, first, inv = np.unique(np.asarray(labels, np.int64), return_index=True, return_inverse=True)
+    return first[inv]
 
 
 def test_noalloc_matches_allocating_entry_point_twice():
@@ -56,3 +65,49 @@ def test_noalloc_rejects_oversized_graph():
     with pytest.raises(UrsaGpuError, match="at most 4194304"):
         _lib.check(_lib.load().ursa_gpu_connected_components_weak_noalloc(g.handle, out.data_ptr(), None))
     assert int(out.abs().sum()) == 0  # nothing was written
+
+
+def test_noalloc_on_callers_stream():
+    import torch
+
+    from ursa_b200 import Topology, algo, gen
+
+    n, s, d = gen.rmat(15, 16, 4)
+    g = Topology.build(n, s, d)
+    ref = algo.connected_components_weak(g)
+    st = torch.cuda.Stream(device="cuda:0")
+    assert np.array_equal(_noalloc_labels(g, n, st), ref)
+    assert np.array_equal(_noalloc_labels(g, n, st), ref)
+
+
+def test_noalloc_at_the_node_limit_matches_oracle(orc):
+    """Exactly 4,194,304 nodes (R-MAT scale 22, seed 2): the last entry of the
+    scratch array is used; the partition equals the oracle's."""
+    from ursa_b200 import Topology, gen
+
+    n, s, d = gen.rmat(22, 16, 2)
+    assert n == 1 << 22
+    g = Topology.build(n, s, d)
+    ref = _canon(orc.connected_components_weak(orc.Topology(n, s, d)))
+    assert np.array_equal(_noalloc_labels(g, n), ref)
+    assert np.array_equal(_noalloc_labels(g, n), ref)
+
+
+def test_noalloc_selects_the_topologys_device():
+    """With another device current on the calling thread, the call still runs
+    on the topology's device (needs two visible GPUs)."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible GPUs")
+    from ursa_b200 import Topology, algo, gen
+
+    n, s, d = gen.rmat(12, 16, 1)
+    g = Topology.build(n, s, d)  # on device 0
+    ref = algo.connected_components_weak(g)
+    st = torch.cuda.Stream(device="cuda:0")
+    torch.cuda.set_device(1)
+    try:
+        assert np.array_equal(_noalloc_labels(g, n, st), ref)
+    finally:
+        torch.cuda.set_device(0)

@@ -7,8 +7,10 @@
 // arena and forbids allocations it does not make.  This entry point needs
 // only memory that exists before the call: the topology (built earlier), the
 // caller's output buffer, and one scratch array declared at file scope
-// below, which every GPU that loads this library holds until the process
-// exits.
+// below.  The array is part of this file's device code: a GPU gets its copy
+// when that code is loaded on it -- with CUDA's default lazy loading, at the
+// first call of this entry point on that GPU -- and keeps it until the
+// process exits.
 #include <mutex>
 
 #include "topo.cuh"
@@ -28,13 +30,17 @@ std::mutex g_scratch_mu;
 uint32_t* g_scratch_addr[64] = {};
 
 // The array's name is a host-side stand-in in host code; the device address
-// is looked up once per device, with that device current.
+// is looked up once per device, with that device current.  The lookup leaves
+// the calling thread's current device as it found it.
 uint32_t* scratch_on(int device) {
   std::lock_guard<std::mutex> g(g_scratch_mu);
   if (!g_scratch_addr[device]) {
+    int prev = 0;
+    UG_CUDA(cudaGetDevice(&prev));
     UG_CUDA(cudaSetDevice(device));
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_cc_scratch);
+    cudaSetDevice(prev);
     if (e != cudaSuccess || !p)
       throw ug::Error(URSA_GPU_ECUDA, std::string("cudaGetSymbolAddress(scratch) failed: ") +
                                           cudaGetErrorString(e));
@@ -60,7 +66,11 @@ extern "C" int ursa_gpu_connected_components_weak_noalloc(ursa_gpu_topo* t, uint
     UG_CHECK(d_labels, URSA_GPU_EINVAL, "d_labels is NULL");
     UG_CHECK(ti->device >= 0 && ti->device < 64, URSA_GPU_EINVAL, "device index out of range");
     uint32_t* parent = scratch_on(ti->device);
-    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream(ti->device);
+    // like every other entry point: the topology's device becomes current on
+    // this thread, so the launches below go to that device even when the
+    // caller's stream is given and another device was current
+    cudaStream_t s = thread_stream(ti->device);
+    if (stream) s = (cudaStream_t)stream;
     // every entry of the shared array that the kernels read is rewritten first
     cc_weak_with_parent(ti, parent, d_labels, s);
     UG_CUDA(cudaStreamSynchronize(s));
