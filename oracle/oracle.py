@@ -53,6 +53,8 @@ def lib():
         L.orc_pagerank.argtypes = [P, f64, u32, f64, P]
         L.orc_pagerank_weighted.restype = u32
         L.orc_pagerank_weighted.argtypes = [P, P, f64, u32, f64, P]
+        L.orc_pagerank_deltas.restype = u32
+        L.orc_pagerank_deltas.argtypes = [P, u32]
         L.orc_bfs_distances.argtypes = [P, u32, i32, P]
         L.orc_shortest_path.restype = i64
         L.orc_shortest_path.argtypes = [P, u32, u32, i32, P]
@@ -152,6 +154,13 @@ def pagerank(t: Topology, damping=0.85, max_iter=30, tol=1e-6, return_iters=Fals
     out = np.empty(t.n, np.float64)
     it = lib().orc_pagerank(t._h, damping, max_iter, tol, _p(out))
     return (out, it) if return_iters else out
+
+
+def pagerank_deltas() -> np.ndarray:
+    """L1 residual of every iteration of this thread's last pagerank call."""
+    buf = np.empty(4096, np.float64)
+    k = lib().orc_pagerank_deltas(_p(buf), buf.size)
+    return buf[: min(k, buf.size)].copy()
 
 
 def pagerank_weighted(t: Topology, weights, damping=0.85, max_iter=30, tol=1e-6, return_iters=False):

@@ -440,6 +440,19 @@ static double l1_delta(const double *a, const double *b, uint64_t n) {
   return s;
 }
 
+/* Per-iteration L1 residuals of this thread's last power_iterate call (test
+ * infrastructure: lets a test show that a differing iteration count sits
+ * next to tol).  Not part of the reference. */
+#define ORC_MAX_DELTAS 4096u
+static __thread double g_deltas[ORC_MAX_DELTAS];
+static __thread uint32_t g_n_deltas;
+
+uint32_t orc_pagerank_deltas(double *out, uint32_t cap) {
+  uint32_t k = g_n_deltas < cap ? g_n_deltas : cap;
+  for (uint32_t i = 0; i < k; i++) out[i] = g_deltas[i];
+  return g_n_deltas;
+}
+
 /* power_iterate (pagerank.rs:63-94). Returns iterations run; the final
  * rank vector (no renormalisation) is copied to out. */
 static uint32_t power_iterate(uint64_t n, double d, uint32_t max_iter, double tol,
@@ -451,6 +464,7 @@ static uint32_t power_iterate(uint64_t n, double d, uint32_t max_iter, double to
   double *next = (double *)calloc(n, sizeof(double));
   for (uint64_t i = 0; i < n; i++) rank[i] = 1.0 / nf;
   uint32_t it;
+  g_n_deltas = 0;
   for (it = 0; it < max_iter;) {
     double dangling_mass = 0.0;
     for (uint64_t i = 0; i < n_dangling; i++) dangling_mass += rank[dangling[i]];
@@ -461,6 +475,8 @@ static uint32_t power_iterate(uint64_t n, double d, uint32_t max_iter, double to
     ctx->d = d;
     par_ranges(n, par_threads_for(work), sweep, ctx);
     double delta = l1_delta(next, rank, n);
+    if (it < ORC_MAX_DELTAS) g_deltas[it] = delta;
+    g_n_deltas = it + 1 < ORC_MAX_DELTAS ? it + 1 : ORC_MAX_DELTAS;
     double *tmp = rank;
     rank = next;
     next = tmp;

@@ -63,6 +63,9 @@ uint32_t orc_pagerank(orc_topo *t, double damping, uint32_t max_iter,
 uint32_t orc_pagerank_weighted(orc_topo *t, const double *weights,
                                double damping, uint32_t max_iter, double tol,
                                double *out);
+/* The L1 residual of each iteration of this thread's last pagerank call
+ * (up to cap of them); returns how many iterations ran. */
+uint32_t orc_pagerank_deltas(double *out, uint32_t cap);
 void orc_bfs_distances(orc_topo *t, uint32_t source, int dir, int32_t *out);
 /* Path into path_out (capacity n); returns its length, or -1 for None. */
 int64_t orc_shortest_path(orc_topo *t, uint32_t source, uint32_t target,

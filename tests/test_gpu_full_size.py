@@ -1,0 +1,180 @@
+"""Parity at the benchmarked sizes, against the oracle on the same inputs.
+
+C2: R-MAT scale 22 (4,194,304 nodes, edge factor 16, a/b/c = .57/.19/.19,
+seed 2, self-loops and duplicates removed -> 65,243,929 edges), the graph the
+PageRank benchmark runs on.  C3: n = 2^20 nodes with Poisson(16) out-degrees
+and uniform targets (seed 3, multiplicity and self-loops kept), f32 weights
+uniform in [1, 10) widened exactly to f64.
+
+Bars (the same as the small-case tests):
+  * CSR and transpose: byte-identical offsets, targets and edge ids
+    (topology.rs:54-187, :307-348);
+  * weak components: the same partition once the oracle's union-find labels
+    are mapped to each component's minimum member (components.rs:58-68);
+  * BFS levels from seeded sources: exact (bfs.rs:18-42);
+  * Dijkstra distances: bit-exact f64 (bfs.rs:126-166);
+  * PageRank (pagerank.rs:98-169): the same iteration count as the oracle --
+    a count that differs by one is accepted only where the oracle's L1
+    residual at the earlier count lies within NEAR_TOL of tol (stated and
+    asserted) -- with L1 <= 1e-6 and max relative error <= 2e-6 against the
+    f64 oracle; at a fixed iteration count the same error bars.
+"""
+
+import concurrent.futures as cf
+
+import numpy as np
+import pytest
+
+from test_gpu_pagerank import L1_FIXED, MAXREL_FIXED, NEAR_TOL, errors
+
+pytestmark = pytest.mark.gpu
+
+DAMPING, TOL, MAX_ITER = 0.85, 1e-6, 100
+
+
+def canon(labels):
+    _, first, inv = np.unique(np.asarray(labels, np.int64), return_index=True, return_inverse=True)
+    return first[inv]
+
+
+@pytest.fixture(scope="module")
+def c2(orc):
+    from ursa_b200 import Topology, gen
+
+    n, s, d = gen.rmat(22, 16, 2)
+    g = Topology.build(n, s, d)
+    o = orc.Topology(n, s, d)
+    yield n, s, d, g, o
+    g.free()
+
+
+@pytest.fixture(scope="module")
+def c3(orc):
+    from ursa_b200 import Topology, gen
+
+    n, s, d = gen.poisson(1 << 20, 16.0, 3)
+    w = gen.weights_f32(s.size, 1.0, 10.0, 3).astype(np.float64)
+    g = Topology.build(n, s, d)
+    o = orc.Topology(n, s, d)
+    yield n, s, d, w, g, o
+    g.free()
+
+
+def check_converged(orc, got, ref, it_gpu, it_ref):
+    l1, maxrel = errors(got, ref)
+    if it_gpu != it_ref:
+        assert abs(it_gpu - it_ref) == 1, (it_gpu, it_ref)
+        deltas = orc.pagerank_deltas()
+        d = deltas[min(it_gpu, it_ref) - 1]
+        assert abs(d - TOL) <= NEAR_TOL * TOL, (it_gpu, it_ref, d)
+        assert l1 <= 3 * TOL and maxrel <= 1e-3, (l1, maxrel)
+    else:
+        assert l1 <= L1_FIXED and maxrel <= MAXREL_FIXED, (l1, maxrel)
+
+
+def test_c2_csr_and_transpose_byte_identical(c2):
+    n, s, d, g, o = c2
+    assert s.size == 65_243_929
+    for mine, ref in ((g.out(), o.csr("out")), (g.incoming(), o.csr("in"))):
+        assert np.array_equal(mine.offsets, ref[0])
+        assert np.array_equal(mine.targets, ref[1])
+        assert np.array_equal(mine.edge_ids, ref[2])
+
+
+def test_c2_pagerank_to_tol(orc, c2):
+    from ursa_b200 import PageRankStats, algo
+
+    n, s, d, g, o = c2
+    st = PageRankStats()
+    got = algo.pagerank(g, damping=DAMPING, max_iter=MAX_ITER, tol=TOL, stats=st)
+    ref, it = orc.pagerank(o, DAMPING, MAX_ITER, TOL, return_iters=True)
+    check_converged(orc, got, ref, st.iterations, it)
+    assert st.last_delta < TOL
+
+
+def test_c2_pagerank_fixed_iterations(orc, c2):
+    from ursa_b200 import PageRankStats, algo
+
+    n, s, d, g, o = c2
+    st = PageRankStats()
+    got = algo.pagerank(g, damping=DAMPING, max_iter=20, tol=0.0, stats=st)
+    ref, it = orc.pagerank(o, DAMPING, 20, 0.0, return_iters=True)
+    assert st.iterations == it == 20
+    l1, maxrel = errors(got, ref)
+    assert l1 <= L1_FIXED and maxrel <= MAXREL_FIXED, (l1, maxrel)
+
+
+def test_c2_connected_components_partition(orc, c2):
+    from ursa_b200 import algo
+
+    n, s, d, g, o = c2
+    got = algo.connected_components_weak(g)
+    ref = orc.connected_components_weak(o)
+    assert np.array_equal(got, canon(ref))
+
+
+def _c2_sources(orc, o, n, k):
+    outdeg = orc.degree(o, "out")
+    have_out = np.flatnonzero(outdeg > 0)
+    return [int(have_out[i]) for i in orc.sample_indices(have_out.size, k, 2)]
+
+
+def test_c2_bfs_distances_exact(orc, c2):
+    from ursa_b200 import algo
+
+    n, s, d, g, o = c2
+    srcs = _c2_sources(orc, o, n, 8)
+    with cf.ThreadPoolExecutor(8) as ex:  # the oracle call releases the GIL
+        refs = list(ex.map(lambda x: orc.bfs_distances(o, x, "out"), srcs))
+    for x, ref in zip(srcs, refs):
+        assert np.array_equal(algo.bfs_distances(g, x, "out"), ref), x
+
+
+def test_c2_bfs_distances_multi_64_sources_exact(orc, c2):
+    from ursa_b200 import algo
+
+    n, s, d, g, o = c2
+    srcs = _c2_sources(orc, o, n, 64)
+    got = algo.bfs_distances_multi(g, srcs, "out")
+    with cf.ThreadPoolExecutor(8) as ex:
+        refs = list(ex.map(lambda x: orc.bfs_distances(o, x, "out"), srcs))
+    for i, ref in enumerate(refs):
+        assert np.array_equal(got[i], ref), srcs[i]
+
+
+def test_c3_pagerank_weighted(orc, c3):
+    from ursa_b200 import PageRankStats, algo
+
+    n, s, d, w, g, o = c3
+    st = PageRankStats()
+    got = algo.pagerank_weighted(g, w, damping=DAMPING, max_iter=MAX_ITER, tol=TOL, stats=st)
+    ref, it = orc.pagerank_weighted(o, w, DAMPING, MAX_ITER, TOL, return_iters=True)
+    check_converged(orc, got, ref, st.iterations, it)
+    got = algo.pagerank_weighted(g, w, damping=DAMPING, max_iter=15, tol=0.0)
+    ref = orc.pagerank_weighted(o, w, DAMPING, 15, 0.0)
+    l1, maxrel = errors(got, ref)
+    assert l1 <= L1_FIXED and maxrel <= MAXREL_FIXED, (l1, maxrel)
+
+
+def test_c3_pagerank_plain(orc, c3):
+    from ursa_b200 import PageRankStats, algo
+
+    n, s, d, w, g, o = c3
+    st = PageRankStats()
+    got = algo.pagerank(g, damping=DAMPING, max_iter=MAX_ITER, tol=TOL, stats=st)
+    ref, it = orc.pagerank(o, DAMPING, MAX_ITER, TOL, return_iters=True)
+    check_converged(orc, got, ref, st.iterations, it)
+
+
+def test_c3_dijkstra_bit_exact(orc, c3):
+    from ursa_b200 import algo
+
+    n, s, d, w, g, o = c3
+    outdeg = orc.degree(o, "out")
+    have_out = np.flatnonzero(outdeg > 0)
+    srcs = [int(have_out[i]) for i in orc.sample_indices(have_out.size, 2, 3)]
+    with cf.ThreadPoolExecutor(2) as ex:
+        refs = list(ex.map(lambda x: orc.dijkstra_distances(o, w, x, "out"), srcs))
+    for x, ref in zip(srcs, refs):
+        got = algo.dijkstra_distances(g, w, x, "out")
+        assert np.array_equal(got.view(np.uint64), ref.view(np.uint64)), x

@@ -5,10 +5,13 @@ accumulation and keeps the update, residual and dangling mass in f64.
 Tolerances (stated here, asserted per run):
   * fixed iteration count (tol = 0): max relative error <= 2e-6 and
     L1 error <= 1e-6;
-  * convergence runs (tol > 0): the iteration count may differ by one when
-    the f64 residual sits next to tol; then L1 <= 3 * tol and max relative
-    error <= 1e-3 (one extra power step); with equal counts the fixed-count
-    bound applies.
+  * convergence runs (tol > 0): the same iteration count as the oracle and
+    the fixed-count bound.  The residual is summed exactly on the device
+    (128-bit fixed point, each term truncated at 2^-96), so a count may
+    differ by one only where the oracle's own residual at the earlier count
+    lies within NEAR_TOL (relative) of tol -- the f32 shares move the device
+    residual by far less than that; such a case is then held to L1 <= 3 * tol
+    and max relative error <= 1e-3 (one power step apart).
 """
 
 import numpy as np
@@ -20,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 MAXREL_FIXED = 2e-6
 L1_FIXED = 1e-6
+NEAR_TOL = 1e-3
 
 
 def errors(got, ref):
@@ -41,6 +45,7 @@ def run_pair(orc, n, s, d, damping=0.85, max_iter=30, tol=1e-6, weights=None):
     else:
         got = algo.pagerank_weighted(g, weights, damping=damping, max_iter=max_iter, tol=tol, stats=st)
         ref, it = orc.pagerank_weighted(o, weights, damping, max_iter, tol, return_iters=True)
+    run_pair.deltas = orc.pagerank_deltas()  # the oracle's residual per iteration
     return got, ref, st.iterations, it
 
 
@@ -50,7 +55,9 @@ def check(got, ref, it_gpu, it_ref, tol):
         assert it_gpu == it_ref
         assert l1 <= L1_FIXED and maxrel <= MAXREL_FIXED, (l1, maxrel)
     else:
-        assert abs(it_gpu - it_ref) <= 1, (it_gpu, it_ref)
+        assert abs(it_gpu - it_ref) == 1, (it_gpu, it_ref)
+        d = run_pair.deltas[min(it_gpu, it_ref) - 1]
+        assert abs(d - tol) <= NEAR_TOL * tol, (it_gpu, it_ref, d)
         assert l1 <= 3 * tol and maxrel <= 1e-3, (l1, maxrel)
 
 

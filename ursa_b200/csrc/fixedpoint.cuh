@@ -68,23 +68,4 @@ __device__ __forceinline__ FxPair fx_ldcg(const FxPair* p) {
 __device__ __forceinline__ u128 fx_delta(const FxPair& p) { return ((u128)p.v[1] << 64) | p.v[0]; }
 __device__ __forceinline__ u128 fx_dang(const FxPair& p) { return ((u128)p.v[3] << 64) | p.v[2]; }
 
-// 64-bit form for sums whose every partial is known to stay below 64 (all
-// terms non-negative and the total bounded, e.g. a PageRank residual <= 2):
-// v -> floor(v * 2^58), saturating; error below 2^-58 per term.
-__device__ __forceinline__ unsigned long long fx64_of(double v) {
-  const uint64_t b = (uint64_t)__double_as_longlong(v);
-  const int e = (int)((b >> 52) & 0x7ff);
-  if (e == 0) return 0;
-  const uint64_t mant = (b & 0xFFFFFFFFFFFFFull) | (1ull << 52);
-  const int sh = e - 1075 + 58;  // v * 2^58 = mant * 2^sh
-  if (sh >= 11) return ~0ull;
-  if (sh >= 0) return mant << sh;
-  if (sh <= -53) return 0;
-  return mant >> -sh;
-}
-
-__device__ __forceinline__ double fx64_value(unsigned long long x) {
-  return __dmul_rn(__ull2double_rn(x), 0x1p-58);
-}
-
 }  // namespace ug

@@ -12,25 +12,46 @@
 //
 // B200 design.
 //  * Arithmetic: the per-edge share x[v] = rank[v]/divisor[v] is stored as
-//    f32 and each row sums its shares with Kahan-compensated f32; the update,
-//    L1 residual, dangling mass and the ranks are f64.
-//  * Execution CSR (built once per topology, cached): a copy of the in-CSR
-//    with node ids relabelled by in-degree, highest first.  Rows of similar
-//    degree become contiguous, so each degree class gets a fixed group width
-//    (1..32 lanes per row, about four edges per lane) and no warp diverges on
-//    row lengths.  On R-MAT graphs in- and out-degree go together, so the
-//    smallest ids are also the most-gathered shares: the first kHot of them
-//    are copied into shared memory every iteration (about half of all gathers
-//    at R-MAT-22), taking them off L2.  Ranks return to the caller's ids at
-//    the end.
-//  * Work units: a unit is 32/G consecutive rows of a class with group width
-//    G, or a kHubChunk-edge chunk of a hub row (in-degree > kHubDeg).  Warps
-//    take units round-robin and never wait for each other inside an
-//    iteration; a hub's chunk sums are combined in chunk order by whichever
-//    chunk arrives last (an arrival counter, no waiting).
-//  * One bounded grid barrier per iteration.  Every reduction has a fixed
-//    order, so runs are bit-reproducible.
+//    f32 and each row sums its shares with Kahan-compensated f32 (pieces of a
+//    row combined with TwoSum); the update, the L1 residual, the dangling mass
+//    and the ranks are f64.  Residual and dangling sums are 128-bit fixed point
+//    (fixedpoint.cuh): exact, so the result does not depend on which thread
+//    summed which row.
+//  * Execution layout (built once per topology, cached).  Nodes are relabelled
+//    by in-degree, highest first; on skewed graphs the most-gathered shares
+//    then have the smallest ids.  The relabelled source ids are cut into
+//    segments of kSegW ids -- one shared-memory slice of shares (192 KB).
+//      - Heavy rows (in-degree > kDirect): each row's in-edges are grouped by
+//        source segment (stable, in-CSR order inside a segment) and cut into
+//        pieces of at most kPiece edges.  The first S segments (chosen per
+//        graph: the leading segments whose pieces average >= 3 edges) keep
+//        16-bit ids local to their segment; the remaining "far" sources keep
+//        32-bit ids.  Within a segment, pieces are sorted by length and packed
+//        32 to a chunk in sliced-ELL order: lane l's ids sit in column blocks
+//        of V ids, so each lane loads V ids with one vector load and a warp
+//        reads 512 (or 128) contiguous bytes per instruction, with no
+//        per-edge bounds test (short pieces are padded with an id whose share
+//        is zero).
+//      - Light rows (1..kDirect in-edges): 32 consecutive rows to a chunk,
+//        one lane per row, 32-bit ids in the same order.
+//  * One iteration:
+//      phase A -- every chunk once.  A CTA owns a contiguous range of the
+//        chunk list (split by a cost model); its warps take chunks from a
+//        block counter.  Segment chunks gather from the slice in shared
+//        memory, which the CTA loads with cp.async.bulk (completion on an
+//        mbarrier, bounded wait) when it moves to another segment; far chunks
+//        gather from L2; light chunks from the segment-0 slice or L2.  A light
+//        row is finished by its lane; a piece writes its partial sum to its
+//        slot.
+//      grid barrier;
+//      phase B -- each heavy row combines its slots in slot order (segment,
+//        then piece) and is finished; rows with many slots take a warp.
+//      grid barrier whose last block sums the residual and dangling mass.
+//    Bounded waits everywhere (grid barriers and mbarrier waits give up after
+//    5 s, set an error flag the host turns into URSA_GPU_ETIMEOUT).
+#include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "fixedpoint.cuh"
 #include "primitives.cuh"
@@ -41,40 +62,58 @@ namespace ug {
 namespace {
 constexpr int kPrBlock = 1024;
 constexpr int kPrWarps = kPrBlock / 32;
-constexpr uint32_t kHubDeg = 1024;    // in-degree above which a row is chunked
-constexpr uint32_t kHubChunk = 2048;  // edges per hub chunk (64 per lane)
-constexpr int kHot = 32768;           // shares cached in shared memory (128 KB)
-constexpr int kClasses = 7;           // hub, G = 32, 16, 8, 4, 2, 1
-constexpr int kBatchWide = 8;         // loads in flight per lane, 32-lane rows
-constexpr int kBatchHub = 16;         // loads in flight per lane, hub chunks
-constexpr int kUnitsPerGrab = 8;      // units a warp takes from its block's counter
-constexpr uint64_t kBarrierLimitNs = 5000000000ull;  // 5 s per grid barrier wait
+constexpr uint32_t kSegW = 49152;    // source ids per shared-memory slice (192 KB of f32 shares)
+constexpr uint32_t kSegMax = 16;     // segments considered; ids >= kSegMax*kSegW are far
+constexpr uint32_t kBins = kSegMax + 1;
+constexpr uint32_t kPiece = 64;      // max edges per piece of a heavy row
+constexpr uint32_t kDirect = 32;     // rows with at most this many in-edges are light
+constexpr uint32_t kWideSlots = 32;  // heavy rows with more slots are combined by a warp
+constexpr int kMaxGroups = kSegMax + 3;
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
+constexpr uint32_t kPadEid = 0xFFFFFFFFu;
+constexpr uint64_t kWaitLimitNs = 5000000000ull;  // 5 s per bounded wait
+// chunk kinds
+constexpr int kSeg8 = 0, kSeg2 = 1, kFar4 = 2, kFar1 = 3, kLight4 = 4, kLight1 = 5;
+// relative cost per slot (phase-A balance across CTAs): shared-memory
+// gathers are cheap, L2 gathers are not; a chunk's cost is
+// (slots * weight) / 16 + kCostChunk, which keeps the u32 prefix far from
+// overflow (R-MAT-24 totals ~ 6e7)
+constexpr uint32_t kCostSeg = 2, kCostFar = 7, kCostLight = 5, kCostChunk = 6;
 }  // namespace
 
-struct PrClassTable {
-  uint32_t lo[kClasses], hi[kClasses];   // row ranges (new ids)
-  uint32_t unit_begin[kClasses + 1];     // first unit of each class
+struct PrChunk {
+  uint32_t base;   // first element in ids16 (segment kinds) or ids32 (others)
+  uint16_t nblk;   // column blocks of V ids per lane
+  uint8_t kind;
+  uint8_t pad;
 };
 
 struct PrPlan {
-  PrClassTable cls{};
-  uint32_t iso_lo = 0;  // rows [iso_lo, n) are isolated: rank follows in closed form
+  uint32_t H = 0;       // heavy rows [0, H)
   uint32_t zi_lo = 0;   // rows [zi_lo, n) have no in-edges: rank = base every iteration
-  uint32_t n_units = 0, n_hub = 0, n_chunks = 0;
-  DevArray<uint2> hub_unit;            // per hub chunk: {hub index, chunk}
-  DevArray<uint32_t> hub_first, hub_nch;
-  // execution CSR in relabelled ids
-  DevArray<uint32_t> old_of_new, new_of_old;
-  DevArray<uint32_t> off, src, eid;
-  DevArray<uint32_t> outdeg;  // per new id
+  uint32_t iso_lo = 0;  // rows [iso_lo, n) are isolated
+  uint32_t S = 0;       // segments with 16-bit ids
+  uint32_t n_slots = 0, n_chunks = 0, n_groups = 0, n_wide = 0;
+  uint32_t n16 = 0, n32 = 0;  // slots in ids16 / ids32
+  uint32_t group_begin[kMaxGroups + 1] = {};
+  int32_t group_slice[kMaxGroups] = {};
+  DevArray<PrChunk> chunks;
+  DevArray<uint32_t> chunk_slot;   // per chunk x lane: partial slot (pieces) or row (light)
+  DevArray<uint32_t> cost_prefix;  // n_chunks + 1
+  DevArray<uint16_t> ids16;
+  DevArray<uint32_t> ids32, eid16, eid32;
+  DevArray<uint32_t> first_slot;  // H + 1
+  DevArray<uint32_t> wide_rows;
+  DevArray<uint32_t> old_of_new, new_of_old, outdeg;
 };
 
 void pr_plan_free(PrPlan* p) { delete p; }
 uint64_t pr_plan_bytes(const PrPlan* p) {
   if (!p) return 0;
-  return (uint64_t)p->hub_unit.n * sizeof(uint2) +
-         4ull * (p->hub_first.n + p->hub_nch.n + p->old_of_new.n + p->new_of_old.n + p->off.n +
-                 p->src.n + p->eid.n + p->outdeg.n);
+  return (uint64_t)p->chunks.n * sizeof(PrChunk) + 2ull * p->ids16.n +
+         4ull * (p->chunk_slot.n + p->cost_prefix.n + p->ids32.n + p->eid16.n + p->eid32.n +
+                 p->first_slot.n + p->wide_rows.n + p->old_of_new.n + p->new_of_old.n +
+                 p->outdeg.n);
 }
 
 namespace {
@@ -126,81 +165,319 @@ __global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n,
   });
 }
 
-// Class boundaries over the non-increasing degree sequence: bounds[t] =
-// number of rows with degree > thr[t]; bounds[kClasses - 1] = first isolated
-// row (in- and out-degree 0; they end the execution order); bounds[kClasses]
-// = first row without in-edges.
-__global__ void class_bounds_k(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ outdeg,
-                               uint64_t n, uint32_t* __restrict__ bounds) {
-  const uint32_t thr[kClasses - 1] = {kHubDeg, 64u, 32u, 16u, 8u, 4u};
-  for (int t = 0; t < kClasses - 1; t++) {
-    uint64_t lo = 0, hi = n;  // first index with deg <= thr
-    while (lo < hi) {
-      uint64_t mid = (lo + hi) >> 1;
-      if (deg[mid] > thr[t])
-        lo = mid + 1;
-      else
-        hi = mid;
-    }
-    bounds[t] = (uint32_t)lo;
-  }
-  uint64_t lo = 0, hi = n;  // first isolated row
+// Over the non-increasing in-degree sequence: out[0] = rows with in-degree >
+// kDirect (heavy), out[1] = rows with in-edges, out[2] = first isolated row.
+__global__ void row_bounds_k(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ outdeg,
+                             uint64_t n, uint32_t* __restrict__ out) {
+  uint64_t lo = 0, hi = n;
   while (lo < hi) {
-    uint64_t mid = (lo + hi) >> 1;
-    if (deg[mid] != 0 || outdeg[mid] != 0)
-      lo = mid + 1;
-    else
-      hi = mid;
+    const uint64_t mid = (lo + hi) >> 1;
+    if (deg[mid] > kDirect) lo = mid + 1; else hi = mid;
   }
-  bounds[kClasses - 1] = (uint32_t)lo;
+  out[0] = (uint32_t)lo;
   lo = 0;
-  hi = n;  // first row without in-edges
+  hi = n;
   while (lo < hi) {
-    uint64_t mid = (lo + hi) >> 1;
-    if (deg[mid] != 0)
-      lo = mid + 1;
-    else
-      hi = mid;
+    const uint64_t mid = (lo + hi) >> 1;
+    if (deg[mid] != 0) lo = mid + 1; else hi = mid;
   }
-  bounds[kClasses] = (uint32_t)lo;
+  out[1] = (uint32_t)lo;
+  lo = 0;
+  hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (deg[mid] != 0 || outdeg[mid] != 0) lo = mid + 1; else hi = mid;
+  }
+  out[2] = (uint32_t)lo;
 }
 
-__global__ void hub_nch_k(const uint32_t* __restrict__ deg, uint32_t n_hub,
-                          uint32_t* __restrict__ nch) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_hub; i += gridDim.x * blockDim.x)
-    nch[i] = (deg[i] + kHubChunk - 1) / kHubChunk;
+// Per heavy row, its in-edges per source segment (bins 0..kSegMax-1, bin
+// kSegMax = ids beyond); per bin, the edge total and the number of rows with
+// at least one edge there (for the choice of S).
+__global__ void seg_hist_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
+                           uint32_t H, uint32_t* __restrict__ cnt,
+                           unsigned long long* __restrict__ tot) {
+  __shared__ uint32_t hist[kBlock / 32][kBins];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
+  unsigned long long my_edges = 0, my_pairs = 0;  // lane b: totals of bin b
+  for (uint32_t r = gw; r < H; r += nw) {
+    if (lane < (int)kBins) hist[w][lane] = 0;
+    __syncwarp();
+    for (uint32_t e = off[r] + lane; e < off[r + 1]; e += 32)
+      atomicAdd(&hist[w][min(src[e] / kSegW, kSegMax)], 1u);
+    __syncwarp();
+    if (lane < (int)kBins) {
+      const uint32_t c = hist[w][lane];
+      cnt[(uint64_t)r * kBins + lane] = c;
+      my_edges += c;
+      my_pairs += c ? 1 : 0;
+    }
+    __syncwarp();
+  }
+  if (lane < (int)kBins && my_edges) {
+    atomicAdd(&tot[lane], my_edges);
+    atomicAdd(&tot[kBins + lane], my_pairs);
+  }
 }
 
-__global__ void hub_units_k(const uint32_t* __restrict__ first, const uint32_t* __restrict__ nch,
-                            uint32_t n_hub, uint2* __restrict__ units) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_hub; i += gridDim.x * blockDim.x)
-    for (uint32_t c = 0; c < nch[i]; c++) units[first[i] + c] = make_uint2(i, c);
+// Count of heavy row r's edges in merged bin b of S+1 (b == S: far).
+__device__ __forceinline__ uint32_t merged_count(const uint32_t* __restrict__ cnt, uint32_t r,
+                                                 uint32_t b, uint32_t S) {
+  const uint32_t* c = cnt + (uint64_t)r * kBins;
+  if (b < S) return c[b];
+  uint32_t t = 0;
+  for (uint32_t k = S; k < kBins; k++) t += c[k];
+  return t;
+}
+
+__global__ void piece_count_k(const uint32_t* __restrict__ cnt, uint32_t H, uint32_t S,
+                              uint32_t* __restrict__ pc) {
+  const uint64_t total = (uint64_t)H * (S + 1);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(i / (S + 1)), b = (uint32_t)(i % (S + 1));
+    pc[i] = (merged_count(cnt, r, b, S) + kPiece - 1) / kPiece;
+  }
+}
+
+__global__ void first_slot_k(const uint32_t* __restrict__ slot_base, uint32_t H, uint32_t S,
+                             const uint32_t* __restrict__ total, uint32_t* __restrict__ first) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= H; r += gridDim.x * blockDim.x)
+    first[r] = r < H ? slot_base[(uint64_t)r * (S + 1)] : *total;
+}
+
+// Stable grouping of each heavy row's in-edges by merged segment (one warp
+// per row): segpre[r][b] = absolute start of bin b in the grouped arrays.
+__global__ void group_rows_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
+                             const uint32_t* __restrict__ eid, const uint32_t* __restrict__ cnt,
+                             uint32_t H, uint32_t S, uint32_t* __restrict__ segpre,
+                             uint32_t* __restrict__ gsrc, uint32_t* __restrict__ geid) {
+  __shared__ uint32_t cursor[kBlock / 32][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t r = gw; r < H; r += nw) {
+    const uint32_t rb = off[r], re = off[r + 1];
+    uint32_t c = lane <= (int)S ? merged_count(cnt, r, (uint32_t)lane, S) : 0u;
+    uint32_t pre = c;  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, pre, o);
+      if (lane >= o) pre += t;
+    }
+    pre -= c;
+    cursor[w][lane] = rb + pre;
+    if (lane <= (int)S) segpre[(uint64_t)r * (S + 1) + lane] = rb + pre;
+    __syncwarp();
+    for (uint32_t e0 = rb; e0 < re; e0 += 32) {
+      const uint32_t e = e0 + lane;
+      const bool valid = e < re;
+      const uint32_t v = valid ? src[e] : 0u;
+      const uint32_t b = valid ? min(v / kSegW, S) : 31u;
+      const unsigned peers = __match_any_sync(0xffffffffu, b);
+      const uint32_t pos = cursor[w][b] + __popc(peers & lt);
+      __syncwarp();
+      if (valid) {
+        gsrc[pos] = v;
+        geid[pos] = eid[e];
+        if (lane == __ffs(peers) - 1) cursor[w][b] += __popc(peers);
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// One record per piece (slot order = row, bin, piece): sort key (bin, length
+// descending) and (row << 5 | bin).
+__global__ void piece_keys_k(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ slot_base,
+                             uint32_t H, uint32_t S, uint32_t* __restrict__ key,
+                             uint32_t* __restrict__ prs) {
+  const uint64_t total = (uint64_t)H * (S + 1);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(i / (S + 1)), b = (uint32_t)(i % (S + 1));
+    const uint32_t c = merged_count(cnt, r, b, S);
+    const uint32_t sb = slot_base[i];
+    for (uint32_t k = 0, left = c; left > 0; k++) {
+      const uint32_t len = left < kPiece ? left : kPiece;
+      key[sb + k] = (b << 7) | (kPiece - len);
+      prs[sb + k] = (r << 5) | b;
+      left -= len;
+    }
+  }
+}
+
+// bounds[b] = first sorted piece of bin b (b in [0, S+1]).
+__global__ void bin_bounds_k(const uint32_t* __restrict__ skey, uint32_t n_pieces, uint32_t S,
+                             uint32_t* __restrict__ bounds) {
+  const uint32_t b = threadIdx.x;
+  if (b > S + 1) return;
+  uint32_t lo = 0, hi = n_pieces;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((skey[mid] >> 7) < b) lo = mid + 1; else hi = mid;
+  }
+  bounds[b] = lo;
+}
+
+struct GroupDesc {
+  uint32_t chunk_begin, item_begin, item_end;
+  int32_t type;  // 0 segment, 1 far, 2 light
+  uint32_t bin;  // segment (type 0)
+};
+
+__device__ __forceinline__ int group_of(const GroupDesc* g, int ng, uint32_t c) {
+  int k = 0;
+  while (k + 1 < ng && c >= g[k + 1].chunk_begin) k++;
+  return k;
+}
+
+// Chunk shapes: the first item of a chunk is its longest (pieces sorted by
+// length, light rows by in-degree, both descending).
+__global__ void chunk_shape_k(const GroupDesc* __restrict__ groups, int ng, uint32_t n_chunks,
+                              const uint32_t* __restrict__ skey, const uint32_t* __restrict__ deg,
+                              PrChunk* __restrict__ chunks, uint32_t* __restrict__ size16,
+                              uint32_t* __restrict__ size32, uint32_t* __restrict__ cost) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_chunks;
+       c += gridDim.x * blockDim.x) {
+    const GroupDesc g = groups[group_of(groups, ng, c)];
+    const uint32_t j0 = g.item_begin + 32u * (c - g.chunk_begin);
+    const uint32_t len = g.type == 2 ? deg[j0] : kPiece - (skey[j0] & 127u);
+    int kind;
+    uint32_t V;
+    if (g.type == 0) {
+      kind = len >= 16 ? kSeg8 : kSeg2;
+      V = len >= 16 ? 8 : 2;
+    } else if (g.type == 1) {
+      kind = len >= 8 ? kFar4 : kFar1;
+      V = len >= 8 ? 4 : 1;
+    } else {
+      kind = len >= 8 ? kLight4 : kLight1;
+      V = len >= 8 ? 4 : 1;
+    }
+    const uint32_t nblk = (len + V - 1) / V;
+    const uint32_t size = 32u * nblk * V;
+    PrChunk ch;
+    ch.base = 0;
+    ch.nblk = (uint16_t)nblk;
+    ch.kind = (uint8_t)kind;
+    ch.pad = 0;
+    chunks[c] = ch;
+    size16[c] = g.type == 0 ? size : 0u;
+    size32[c] = g.type == 0 ? 0u : size;
+    const uint32_t wk = g.type == 0 ? kCostSeg : (g.type == 1 ? kCostFar : kCostLight);
+    cost[c] = size * wk / 16 + kCostChunk;
+  }
+}
+
+__global__ void chunk_base_k(uint32_t n_chunks, const uint32_t* __restrict__ base16,
+                             const uint32_t* __restrict__ base32, PrChunk* __restrict__ chunks) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_chunks;
+       c += gridDim.x * blockDim.x) {
+    const int kind = chunks[c].kind;
+    chunks[c].base = (kind == kSeg8 || kind == kSeg2) ? base16[c] : base32[c];
+  }
+}
+
+// Fills the sliced-ELL ids (and original edge ids) of every chunk, one warp
+// per chunk; lane l holds item l of the chunk.
+__global__ void chunk_fill_k(const GroupDesc* __restrict__ groups, int ng, uint32_t n_chunks,
+                             const PrChunk* __restrict__ chunks, const uint32_t* __restrict__ skey,
+                             const uint32_t* __restrict__ order, const uint32_t* __restrict__ prs,
+                             const uint32_t* __restrict__ slot_base,
+                             const uint32_t* __restrict__ segpre, const uint32_t* __restrict__ gsrc,
+                             const uint32_t* __restrict__ geid, const uint32_t* __restrict__ off,
+                             const uint32_t* __restrict__ src, const uint32_t* __restrict__ eid,
+                             const uint32_t* __restrict__ deg, uint32_t S, uint64_t n,
+                             uint32_t n_slots, uint16_t* __restrict__ ids16,
+                             uint32_t* __restrict__ eid16, uint32_t* __restrict__ ids32,
+                             uint32_t* __restrict__ eid32, uint32_t* __restrict__ chunk_slot) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = gw; c < n_chunks; c += nw) {
+    const GroupDesc g = groups[group_of(groups, ng, c)];
+    const PrChunk ch = chunks[c];
+    const uint32_t j = g.item_begin + 32u * (c - g.chunk_begin) + (uint32_t)lane;
+    const bool valid = j < g.item_end;
+    const uint32_t V = ch.kind == kSeg8 ? 8u
+                       : ch.kind == kSeg2 ? 2u
+                       : (ch.kind == kFar4 || ch.kind == kLight4) ? 4u : 1u;
+    const uint32_t width = (uint32_t)ch.nblk * V;
+    uint32_t len = 0, start = 0, sub = 0, slot_or_row = g.type == 2 ? kNoRow : n_slots;
+    const uint32_t* ssrc = gsrc;
+    const uint32_t* seid = geid;
+    if (valid) {
+      if (g.type == 2) {
+        len = deg[j];
+        start = off[j];
+        ssrc = src;
+        seid = eid;
+        slot_or_row = j;
+      } else {
+        const uint32_t slot = order[j];
+        const uint32_t pr = prs[slot];
+        const uint32_t r = pr >> 5, b = pr & 31u;
+        const uint64_t rb = (uint64_t)r * (S + 1) + b;
+        len = kPiece - (skey[j] & 127u);
+        start = segpre[rb] + (slot - slot_base[rb]) * kPiece;
+        sub = g.type == 0 ? b * kSegW : 0u;
+        slot_or_row = slot;
+      }
+    }
+    chunk_slot[(uint64_t)c * 32 + lane] = slot_or_row;
+    for (uint32_t col = 0; col < width; col++) {
+      const uint64_t el = (uint64_t)ch.base + ((uint64_t)(col / V) * 32 + lane) * V + (col % V);
+      const bool have = col < len;
+      const uint32_t v = have ? ssrc[start + col] : 0u;
+      const uint32_t e = have ? seid[start + col] : kPadEid;
+      if (g.type == 0) {
+        ids16[el] = have ? (uint16_t)(v - sub) : (uint16_t)kSegW;
+        eid16[el] = e;
+      } else {
+        ids32[el] = have ? v : (uint32_t)n;
+        eid32[el] = e;
+      }
+    }
+  }
+}
+
+__global__ void wide_flag_k(const uint32_t* __restrict__ first, uint32_t H,
+                            uint32_t* __restrict__ flag) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < H; r += gridDim.x * blockDim.x)
+    flag[r] = first[r + 1] - first[r] > kWideSlots ? 1u : 0u;
+}
+
+__global__ void wide_scatter_k(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                               uint32_t H, uint32_t* __restrict__ out) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < H; r += gridDim.x * blockDim.x)
+    if (flag[r]) out[pos[r]] = r;
 }
 
 // ---------------------------------------------------------- iteration kernel
 struct PrArgs {
   uint64_t n;
-  uint32_t hot;                        // shares cached in shared memory (<= kHot)
-  PrClassTable cls;
-  uint32_t n_units;
-  const uint32_t* __restrict__ off;    // execution CSR offsets (new ids)
-  const uint32_t* __restrict__ src;    // execution CSR sources (new ids)
-  const float* __restrict__ w;         // weighted: f32 weight per slot, else null
-  const uint32_t* __restrict__ outdeg;   // unweighted divisor (new ids)
-  const double* __restrict__ out_str;    // weighted divisor (new ids), else null
+  uint32_t H, zi_lo, iso_lo;
+  uint32_t n_chunks, n_groups, n_wide;
+  uint32_t group_begin[kMaxGroups + 1];
+  int32_t group_slice[kMaxGroups];
+  const PrChunk* __restrict__ chunks;
+  const uint32_t* __restrict__ chunk_slot;
+  const uint32_t* __restrict__ cost_prefix;
+  const uint16_t* __restrict__ ids16;
+  const uint32_t* __restrict__ ids32;
+  const float* __restrict__ w16;  // weighted: f32 weight per slot, else null
+  const float* __restrict__ w32;
+  const uint32_t* __restrict__ first_slot;
+  const uint32_t* __restrict__ wide_rows;
+  F2* partial;
+  const uint32_t* __restrict__ outdeg;  // unweighted divisor (new ids)
+  const double* __restrict__ out_str;   // weighted divisor (new ids), else null
   double* rank[2];
   float* x[2];
-  const uint2* __restrict__ hub_unit;
-  const uint32_t* __restrict__ hub_first;
-  const uint32_t* __restrict__ hub_nch;
-  uint32_t n_hub;
-  F2* chunk_part;            // per hub chunk
-  unsigned* hub_cnt;         // per hub: chunk arrivals this iteration
-  ulonglong2* hub_contrib[2];  // per hub: (|next-rank|, dangling next), fixed point
-  ulonglong2* block_part[2];   // per block, fixed point
-  double2* totals;           // [2]: (delta, dangling) published by the barrier
-  uint32_t iso_lo;           // first isolated row
-  uint32_t zi_lo;            // first row without in-edges (<= iso_lo)
+  FxPair* block_part[2];  // per block, fixed point
+  double2* totals;        // [2]: (delta, dangling) published by the barrier
   unsigned* bar_count;
   unsigned* bar_gen;
   int* err;
@@ -217,19 +494,79 @@ struct Fin {
 };
 
 // Per-thread fixed-point accumulators of |next - rank| and of the dangling
-// rows' next ranks (64-bit, scale 2^-58: order-independent; every partial
-// sum is below its total, and the totals are at most 2 and 1).
+// rows' next ranks: 128-bit integers in units of 2^-96 (fixedpoint.cuh), so
+// the sums are exact and order-independent, and each term loses less than
+// 2^-96 -- the L1 residual compared with tol is at least as precise as an
+// f64 sum of the same terms.
 struct Fx {
-  unsigned long long delta, dang;
+  u128 delta, dang;
 };
 
 struct PrSmem {
-  float hot[kHot];
-  ulonglong2 red[kPrWarps];
+  float x[kSegW + 4];  // the loaded slice; [kSegW] is the zero share of padding ids
+  FxPair red[kPrWarps];
+  unsigned long long mbar;
   unsigned gen;
   int last;
-  unsigned next;  // work counter of the block (dynamic unit scheduling)
+  uint32_t n_sub;
+  unsigned ctr[kMaxGroups];
+  uint32_t sub_begin[kMaxGroups], sub_end[kMaxGroups];
+  int32_t sub_slice[kMaxGroups];
 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the mbarrier phase `parity`; false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  if (mbar_try_wait(mbar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(mbar, parity))
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  return true;
+}
+
+// Loads x[seg * kSegW, +kSegW) into the slice with four bulk copies that
+// complete on the block's mbarrier; every thread waits for the phase.  Called
+// by the whole block after a block barrier.  A wait that runs out sets the
+// error flag, then waits once more (bounded) for the copies still in flight.
+__device__ __forceinline__ void load_slice(const PrArgs& a, PrSmem& sm, const float* x, int seg,
+                                           uint32_t& phase) {
+  const uint32_t mbar = smem_u32(&sm.mbar);
+  constexpr uint32_t kPart = kSegW * 4 / 4;  // bytes per copy (a multiple of 16)
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+                 "r"(kSegW * 4)
+                 : "memory");
+    const char* src = reinterpret_cast<const char*>(x + (size_t)seg * kSegW);
+    const uint32_t dst = smem_u32(sm.x);
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+          ::"r"(dst + k * kPart), "l"(src + (size_t)k * kPart), "r"(kPart), "r"(mbar)
+          : "memory");
+  }
+  if (!mbar_wait(mbar, phase)) {
+    atomicExch(a.err, 1);
+    mbar_wait(mbar, phase);
+  }
+  phase ^= 1u;
+}
 
 __device__ __forceinline__ double row_divisor(const PrArgs& a, uint64_t u) {
   return a.out_str ? a.out_str[u] : (double)a.outdeg[u];
@@ -239,11 +576,11 @@ __device__ __forceinline__ void finish_row(const PrArgs& a, uint64_t u, double s
                                            double div, double base, int cur, Fx& f) {
   // next[u] = base + d * contrib(u)   (pagerank.rs:81-83)
   double nx = __dadd_rn(base, __dmul_rn(a.damping, sum));
-  f.delta += fx64_of(fabs(__dsub_rn(nx, old)));
+  f.delta += fx_of(fabs(__dsub_rn(nx, old)));
   a.rank[cur ^ 1][u] = nx;
   bool dangling = !(div > 0.0);
   a.x[cur ^ 1][u] = dangling ? 0.f : (float)(nx / div);
-  if (dangling) f.dang += fx64_of(nx);
+  if (dangling) f.dang += fx_of(nx);
 }
 
 __device__ __forceinline__ void init_row(const PrArgs& a, uint64_t u, double r0, Fx& f) {
@@ -251,7 +588,7 @@ __device__ __forceinline__ void init_row(const PrArgs& a, uint64_t u, double r0,
   double div = row_divisor(a, u);
   bool dangling = !(div > 0.0);
   a.x[0][u] = dangling ? 0.f : (float)(r0 / div);
-  if (dangling) f.dang += fx64_of(r0);
+  if (dangling) f.dang += fx_of(r0);
 }
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
@@ -261,164 +598,213 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
   s = t;
 }
 
-// Share of source v: shared-memory copy for the hottest ids, else global.
-__device__ __forceinline__ float share(const PrArgs& a, const PrSmem& sm, const float* x,
-                                      uint32_t v) {
-  return v < a.hot ? sm.hot[v] : x[v];
+// Share gathers.  far: global; light: the segment-0 slice for ids below
+// kSegW, else global.
+__device__ __forceinline__ float g_far(const float* x, uint32_t v) { return x[v]; }
+__device__ __forceinline__ float g_light(const PrSmem& sm, const float* x, uint32_t v) {
+  return v < kSegW ? sm.x[v] : x[v];
 }
 
-// Sums the shares of edges [b + sub, e) with stride G; B source loads (and
-// then B gathers) in flight per lane.
-template <int G, bool kW, int B>
-__device__ __forceinline__ F2 row_sum(const PrArgs& a, const PrSmem& sm, const float* x, uint32_t b,
-                                      uint32_t e, int sub) {
+// 16-bit local ids, eight per lane per block, gathered from the slice in
+// shared memory (padding id kSegW reads the zero slot); the next block's ids
+// are loaded before this block's gathers.
+template <bool kW>
+__device__ __forceinline__ F2 sum_seg8(const PrArgs& a, const PrSmem& sm, PrChunk ch, int lane) {
+  const uint4* p = reinterpret_cast<const uint4*>(a.ids16 + ch.base) + lane;
   float s = 0.f, c = 0.f;
-  for (uint32_t j = b + sub; j < e; j += B * G) {
-    uint32_t v[B];
+  uint4 nx = __ldcs(p);
+  for (uint32_t b = 0; b < ch.nblk; b++) {
+    const uint4 q = nx;
+    if (b + 1 < ch.nblk) nx = __ldcs(p + (b + 1) * 32);
+    const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+    float v[8];
 #pragma unroll
-    for (int k = 0; k < B; k++) {
-      uint32_t jj = j + k * G;
-      v[k] = jj < e ? __ldcs(a.src + jj) : 0u;
+    for (int k = 0; k < 4; k++) {
+      v[2 * k] = sm.x[w4[k] & 0xFFFFu];
+      v[2 * k + 1] = sm.x[w4[k] >> 16];
     }
-    float sv[B];
-#pragma unroll
-    for (int k = 0; k < B; k++) {
-      uint32_t jj = j + k * G;
-      sv[k] = 0.f;
-      if (jj < e) {
-        sv[k] = share(a, sm, x, v[k]);
-        if (kW) sv[k] = __fmul_rn(sv[k], __ldcs(a.w + jj));
-      }
+    if (kW) {
+      const float4* wp =
+          reinterpret_cast<const float4*>(a.w16 + ch.base) + ((size_t)b * 32 + lane) * 2;
+      const float4 w0 = __ldcs(wp), w1 = __ldcs(wp + 1);
+      v[0] = __fmul_rn(v[0], w0.x);
+      v[1] = __fmul_rn(v[1], w0.y);
+      v[2] = __fmul_rn(v[2], w0.z);
+      v[3] = __fmul_rn(v[3], w0.w);
+      v[4] = __fmul_rn(v[4], w1.x);
+      v[5] = __fmul_rn(v[5], w1.y);
+      v[6] = __fmul_rn(v[6], w1.z);
+      v[7] = __fmul_rn(v[7], w1.w);
     }
 #pragma unroll
-    for (int k = 0; k < B; k++)
-      if (j + k * G < e) kahan_add(s, c, sv[k]);
+    for (int k = 0; k < 8; k++) kahan_add(s, c, v[k]);
   }
   return F2{s, -c};
 }
 
-// Fixed-order reduction over the G lanes of a group; valid in sub == 0.
-template <int G>
-__device__ __forceinline__ F2 group_sum(F2 v) {
+// 16-bit local ids, two per lane per block, two blocks per step.
+template <bool kW>
+__device__ __forceinline__ F2 sum_seg2(const PrArgs& a, const PrSmem& sm, PrChunk ch, int lane) {
+  const uint32_t* p = reinterpret_cast<const uint32_t*>(a.ids16 + ch.base) + lane;
+  float s = 0.f, c = 0.f;
+  for (uint32_t b = 0; b < ch.nblk; b += 2) {
+    const bool two = b + 1 < ch.nblk;
+    const uint32_t q0 = __ldcs(p + b * 32);
+    const uint32_t q1 = two ? __ldcs(p + (b + 1) * 32) : (kSegW | (kSegW << 16));
+    float v[4] = {sm.x[q0 & 0xFFFFu], sm.x[q0 >> 16], sm.x[q1 & 0xFFFFu], sm.x[q1 >> 16]};
+    if (kW) {
+      const float2* wp = reinterpret_cast<const float2*>(a.w16 + ch.base) + (size_t)b * 32 + lane;
+      const float2 w0 = __ldcs(wp);
+      const float2 w1 = two ? __ldcs(wp + 32) : make_float2(0.f, 0.f);
+      v[0] = __fmul_rn(v[0], w0.x);
+      v[1] = __fmul_rn(v[1], w0.y);
+      v[2] = __fmul_rn(v[2], w1.x);
+      v[3] = __fmul_rn(v[3], w1.y);
+    }
+    kahan_add(s, c, v[0]);
+    kahan_add(s, c, v[1]);
+    if (two) {
+      kahan_add(s, c, v[2]);
+      kahan_add(s, c, v[3]);
+    }
+  }
+  return F2{s, -c};
+}
+
+// 32-bit ids, four per lane per block, two blocks per step (eight gathers in
+// flight); kLight selects the segment-0 slice for small ids.
+template <bool kW, bool kLight>
+__device__ __forceinline__ F2 sum_u32x4(const PrArgs& a, const PrSmem& sm, const float* x,
+                                        PrChunk ch, int lane) {
+  const uint4* p = reinterpret_cast<const uint4*>(a.ids32 + ch.base) + lane;
+  const uint32_t pad = (uint32_t)a.n;
+  float s = 0.f, c = 0.f;
+  for (uint32_t b = 0; b < ch.nblk; b += 2) {
+    const bool two = b + 1 < ch.nblk;
+    const uint4 q0 = __ldcs(p + b * 32);
+    const uint4 q1 = two ? __ldcs(p + (b + 1) * 32) : make_uint4(pad, pad, pad, pad);
+    const uint32_t id[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    float v[8];
 #pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) {
-    F2 t{__shfl_down_sync(0xffffffffu, v.hi, o, G), __shfl_down_sync(0xffffffffu, v.lo, o, G)};
+    for (int k = 0; k < 8; k++) v[k] = kLight ? g_light(sm, x, id[k]) : g_far(x, id[k]);
+    if (kW) {
+      const float4* wp = reinterpret_cast<const float4*>(a.w32 + ch.base) + (size_t)b * 32 + lane;
+      const float4 w0 = __ldcs(wp);
+      const float4 w1 = two ? __ldcs(wp + 32) : make_float4(0.f, 0.f, 0.f, 0.f);
+      v[0] = __fmul_rn(v[0], w0.x);
+      v[1] = __fmul_rn(v[1], w0.y);
+      v[2] = __fmul_rn(v[2], w0.z);
+      v[3] = __fmul_rn(v[3], w0.w);
+      v[4] = __fmul_rn(v[4], w1.x);
+      v[5] = __fmul_rn(v[5], w1.y);
+      v[6] = __fmul_rn(v[6], w1.z);
+      v[7] = __fmul_rn(v[7], w1.w);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) kahan_add(s, c, v[k]);
+    if (two) {
+#pragma unroll
+      for (int k = 4; k < 8; k++) kahan_add(s, c, v[k]);
+    }
+  }
+  return F2{s, -c};
+}
+
+// 32-bit ids, one per lane per block, four blocks per step.
+template <bool kW, bool kLight>
+__device__ __forceinline__ F2 sum_u32x1(const PrArgs& a, const PrSmem& sm, const float* x,
+                                        PrChunk ch, int lane) {
+  const uint32_t* p = a.ids32 + ch.base + lane;
+  float s = 0.f, c = 0.f;
+  for (uint32_t b = 0; b < ch.nblk; b += 4) {
+    uint32_t id[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) id[k] = b + k < ch.nblk ? __ldcs(p + (b + k) * 32) : (uint32_t)a.n;
+    float v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = kLight ? g_light(sm, x, id[k]) : g_far(x, id[k]);
+    if (kW) {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        v[k] = __fmul_rn(v[k], b + k < ch.nblk ? __ldcs(a.w32 + ch.base + (size_t)(b + k) * 32 + lane)
+                                               : 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (b + k < ch.nblk) kahan_add(s, c, v[k]);
+  }
+  return F2{s, -c};
+}
+
+template <bool kW>
+__device__ __forceinline__ void run_chunk(const PrArgs& a, const PrSmem& sm, uint32_t c, int cur,
+                                          double base, Fx& f) {
+  const int lane = threadIdx.x & 31;
+  const PrChunk ch = a.chunks[c];
+  const uint32_t slot = __ldg(a.chunk_slot + (size_t)c * 32 + lane);
+  const float* x = a.x[cur];
+  if (ch.kind == kLight4 || ch.kind == kLight1) {
+    double old = 0.0, div = 0.0;
+    if (slot != kNoRow) {
+      old = a.rank[cur][slot];
+      div = row_divisor(a, slot);
+    }
+    const F2 r = ch.kind == kLight4 ? sum_u32x4<kW, true>(a, sm, x, ch, lane)
+                                    : sum_u32x1<kW, true>(a, sm, x, ch, lane);
+    if (slot != kNoRow) finish_row(a, slot, f2_value(r), old, div, base, cur, f);
+    return;
+  }
+  F2 r;
+  switch (ch.kind) {
+    case kSeg8: r = sum_seg8<kW>(a, sm, ch, lane); break;
+    case kSeg2: r = sum_seg2<kW>(a, sm, ch, lane); break;
+    case kFar4: r = sum_u32x4<kW, false>(a, sm, x, ch, lane); break;
+    default: r = sum_u32x1<kW, false>(a, sm, x, ch, lane); break;
+  }
+  a.partial[slot] = r;
+}
+
+// Fixed-order reduction over the 32 lanes; valid in lane 0.
+__device__ __forceinline__ F2 warp_sum_f2(F2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    F2 t{__shfl_down_sync(0xffffffffu, v.hi, o), __shfl_down_sync(0xffffffffu, v.lo, o)};
     v = f2_combine(v, t);
   }
   return v;
 }
 
-// One unit of a row class: 32/G consecutive rows, G lanes per row.
-template <int G, bool kW>
-__device__ __forceinline__ void class_unit(const PrArgs& a, const PrSmem& sm, uint32_t lo,
-                                           uint32_t hi, uint32_t unit, int cur, double base,
-                                           Fx& f) {
-  const int lane = threadIdx.x & 31;
-  const int sub = lane % G;
-  const uint32_t r = lo + unit * (32u / G) + (uint32_t)(lane / G);
-  const bool valid = r < hi;
-  uint32_t b = 0, e = 0;
-  double old = 0.0, div = 0.0;
-  if (valid) {
-    b = a.off[r];
-    e = a.off[r + 1];
-    if (sub == 0) {
-      old = a.rank[cur][r];
-      div = row_divisor(a, r);
-    }
-  }
-  F2 acc = row_sum<G, kW, (G >= 32 ? kBatchWide : 4)>(a, sm, a.x[cur], b, e, sub);
-  acc = group_sum<G>(acc);
-  if (valid && sub == 0) finish_row(a, r, f2_value(acc), old, div, base, cur, f);
-}
-
-template <bool kW>
-__device__ __forceinline__ void hub_unit(const PrArgs& a, const PrSmem& sm, uint32_t unit, int cur,
-                                         int parity, double base) {
-  const int lane = threadIdx.x & 31;
-  const uint2 hu = a.hub_unit[unit];
-  const uint32_t r = a.cls.lo[0] + hu.x;  // hub rows are the first rows
-  const uint32_t rb = a.off[r], re = a.off[r + 1];
-  const uint32_t eb = rb + hu.y * kHubChunk;
-  const uint32_t ee = eb + kHubChunk < re ? eb + kHubChunk : re;
-  F2 acc = row_sum<32, kW, kBatchHub>(a, sm, a.x[cur], eb, ee, lane);
-  acc = group_sum<32>(acc);
-  if (lane == 0) {
-    const uint32_t nch = a.hub_nch[hu.x];
-    bool finish = nch == 1;
-    F2 row = acc;
-    if (!finish) {
-      a.chunk_part[unit] = acc;
-      __threadfence();
-      unsigned arrived = atomicAdd(&a.hub_cnt[hu.x], 1u);
-      if (arrived == nch - 1) {
-        __threadfence();
-        finish = true;
-        const uint32_t first = a.hub_first[hu.x];
-        row = f2_zero();
-        for (uint32_t k = 0; k < nch; k++) {
-          F2 pk;
-          pk.hi = __ldcg(&a.chunk_part[first + k].hi);
-          pk.lo = __ldcg(&a.chunk_part[first + k].lo);
-          row = f2_combine(row, pk);
-        }
-        a.hub_cnt[hu.x] = 0u;
-      }
-    }
-    if (finish) {
-      Fx g{0, 0};
-      finish_row(a, r, f2_value(row), a.rank[cur][r], row_divisor(a, r), base, cur, g);
-      a.hub_contrib[parity][hu.x] = make_ulonglong2(g.delta, g.dang);
-    }
-  }
-}
-
-template <bool kW>
-__device__ __forceinline__ void run_unit(const PrArgs& a, const PrSmem& sm, uint32_t u, int cur,
-                                         int parity, double base, Fx& f) {
-  int c = 0;
-#pragma unroll
-  for (int k = 1; k < kClasses; k++)
-    if (u >= a.cls.unit_begin[k]) c = k;
-  const uint32_t unit = u - a.cls.unit_begin[c];
-  const uint32_t lo = a.cls.lo[c], hi = a.cls.hi[c];
-  switch (c) {
-    case 0: hub_unit<kW>(a, sm, unit, cur, parity, base); break;
-    case 1: class_unit<32, kW>(a, sm, lo, hi, unit, cur, base, f); break;
-    case 2: class_unit<16, kW>(a, sm, lo, hi, unit, cur, base, f); break;
-    case 3: class_unit<8, kW>(a, sm, lo, hi, unit, cur, base, f); break;
-    case 4: class_unit<4, kW>(a, sm, lo, hi, unit, cur, base, f); break;
-    case 5: class_unit<2, kW>(a, sm, lo, hi, unit, cur, base, f); break;
-    default: class_unit<1, kW>(a, sm, lo, hi, unit, cur, base, f); break;
-  }
+// Partial sums written by other blocks in this iteration: read through L2.
+__device__ __forceinline__ F2 ldcg_f2(const F2* p) {
+  const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+  return F2{v.x, v.y};
 }
 
 // Block sum of the fixed-point accumulators; result valid in thread 0.
-__device__ __forceinline__ Fx block_sum_fx(Fx v, ulonglong2* sh) {
+__device__ __forceinline__ Fx block_sum_fx(Fx v, FxPair* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    v.delta += __shfl_down_sync(0xffffffffu, v.delta, o);
-    v.dang += __shfl_down_sync(0xffffffffu, v.dang, o);
+    v.delta += shfl_down_u128(v.delta, o);
+    v.dang += shfl_down_u128(v.dang, o);
   }
   __syncthreads();
-  if (lane == 0) sh[w] = make_ulonglong2(v.delta, v.dang);
+  if (lane == 0) sh[w] = fx_pack(v.delta, v.dang);
   __syncthreads();
   Fx r{0, 0};
   if (threadIdx.x == 0)
     for (int i = 0; i < kPrWarps; i++) {
-      r.delta += sh[i].x;
-      r.dang += sh[i].y;
+      r.delta += fx_delta(sh[i]);
+      r.dang += fx_dang(sh[i]);
     }
   return r;
 }
 
-// Bounded grid barrier whose last-arriving block sums the fixed-point
-// partials of parity p (block partials and hub contributions; exact, so the
-// result does not depend on which block arrives last or which warp did which
-// unit), adds `extra` (the closed-form terms of the rows without in-edges)
-// and publishes the totals; every block returns them.  A wait longer than
-// kBarrierLimitNs sets the error flag and returns.
+// Bounded grid barrier whose last-arriving block sums the fixed-point block
+// partials of parity p (exact, so the result does not depend on which block
+// arrives last), adds `extra` (the closed-form terms of the rows without
+// in-edges) and publishes the totals; every block returns them.  A wait
+// longer than kWaitLimitNs sets the error flag and returns.
 __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm, Fin extra) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -431,19 +817,14 @@ __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm
     __threadfence();
     Fx acc{0, 0};
     for (uint32_t i = threadIdx.x; i < gridDim.x; i += kPrBlock) {
-      const ulonglong2 v = __ldcg(&a.block_part[p][i]);
-      acc.delta += v.x;
-      acc.dang += v.y;
-    }
-    for (uint32_t i = threadIdx.x; i < a.n_hub; i += kPrBlock) {
-      const ulonglong2 v = __ldcg(&a.hub_contrib[p][i]);
-      acc.delta += v.x;
-      acc.dang += v.y;
+      const FxPair v = fx_ldcg(&a.block_part[p][i]);
+      acc.delta += fx_delta(v);
+      acc.dang += fx_dang(v);
     }
     const Fx r = block_sum_fx(acc, sm.red);
     if (threadIdx.x == 0) {
-      a.totals[p] = make_double2(__dadd_rn(fx64_value(r.delta), extra.delta),
-                                 __dadd_rn(fx64_value(r.dang), extra.dang));
+      a.totals[p] = make_double2(__dadd_rn(fx_value(r.delta), extra.delta),
+                                 __dadd_rn(fx_value(r.dang), extra.dang));
       __threadfence();
       atomicExch(a.bar_count, 0u);
       __threadfence();
@@ -453,7 +834,7 @@ __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm
     const uint64_t t0 = global_ns();
     while (*(volatile unsigned*)a.bar_gen == sm.gen) {
       __nanosleep(32);
-      if (global_ns() - t0 > kBarrierLimitNs) {
+      if (global_ns() - t0 > kWaitLimitNs) {
         atomicExch(a.err, 1);
         break;
       }
@@ -464,17 +845,6 @@ __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm
   __syncthreads();
   const double2 t = __ldcg(&a.totals[p]);
   return Fin{t.x, t.y};
-}
-
-__device__ __forceinline__ void load_hot(const PrArgs& a, PrSmem& sm, int cur) {
-  const float* __restrict__ x = a.x[cur];
-  const uint32_t n4 = a.hot / 4;
-  const float4* x4 = reinterpret_cast<const float4*>(x);
-  float4* h4 = reinterpret_cast<float4*>(sm.hot);
-#pragma unroll 4
-  for (uint32_t i = threadIdx.x; i < n4; i += kPrBlock) h4[i] = __ldcg(x4 + i);
-  for (uint32_t i = n4 * 4 + threadIdx.x; i < a.hot; i += kPrBlock) sm.hot[i] = __ldcg(x + i);
-  __syncthreads();
 }
 
 // Sources without in-edges (rows [zi_lo, iso_lo)): their rank is `rank`
@@ -488,44 +858,64 @@ __device__ __forceinline__ void sources_without_in_edges(const PrArgs& a, double
     const double div = row_divisor(a, u);
     const bool dangling = !(div > 0.0);
     a.x[buf][u] = dangling ? 0.f : (float)(rank / div);
-    if (dangling) f.dang += fx64_of(rank);
+    if (dangling) f.dang += fx_of(rank);
   }
 }
 
+// This block's contiguous range of the chunk list (by the cost prefix), cut
+// at group boundaries into sub-ranges, each with the slice it needs.
+__device__ __forceinline__ void block_ranges(const PrArgs& a, PrSmem& sm) {
+  if (threadIdx.x != 0) return;
+  const uint64_t total = a.n_chunks ? a.cost_prefix[a.n_chunks] : 0;
+  auto first_of = [&](uint32_t blk) -> uint32_t {  // first chunk whose start maps to >= blk
+    if (total == 0) return a.n_chunks;
+    uint32_t lo = 0, hi = a.n_chunks;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if ((uint64_t)a.cost_prefix[mid] * gridDim.x / total < blk) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+  };
+  const uint32_t lo = first_of(blockIdx.x), hi = first_of(blockIdx.x + 1);
+  uint32_t k = 0;
+  for (uint32_t g = 0; g < a.n_groups; g++) {
+    const uint32_t b = max(lo, a.group_begin[g]), e = min(hi, a.group_begin[g + 1]);
+    if (b < e) {
+      sm.sub_begin[k] = b;
+      sm.sub_end[k] = e;
+      sm.sub_slice[k] = a.group_slice[g];
+      k++;
+    }
+  }
+  sm.n_sub = k;
+}
+
 template <bool kW>
-__global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   PrSmem& sm = *reinterpret_cast<PrSmem*>(smem_raw);
   const double nf = (double)a.n;
+  const int lane = threadIdx.x & 31;
   const uint32_t gwarp = blockIdx.x * kPrWarps + (threadIdx.x >> 5);
   const uint32_t nwarps = gridDim.x * kPrWarps;
-  const int lane = threadIdx.x & 31;
+  const uint64_t gtid = (uint64_t)blockIdx.x * kPrBlock + threadIdx.x;
+  const uint64_t nthr = (uint64_t)gridDim.x * kPrBlock;
+  if (threadIdx.x < 4) sm.x[kSegW + threadIdx.x] = 0.f;
+  if (threadIdx.x == 0)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sm.mbar)), "r"(1)
+                 : "memory");
+  block_ranges(a, sm);
+  if (threadIdx.x == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
+  uint32_t phase = 0;
   // ---- prologue: rank_0 = 1/n, shares, dangling mass of rank_0
   {
     Fx f{0, 0};
     const double r0 = 1.0 / nf;
-    for (uint32_t u = gwarp; u < a.n_units; u += nwarps) {
-      int c = 0;
-#pragma unroll
-      for (int k = 1; k < kClasses; k++)
-        if (u >= a.cls.unit_begin[k]) c = k;
-      const uint32_t unit = u - a.cls.unit_begin[c];
-      if (c == 0) {
-        const uint2 hu = a.hub_unit[unit];
-        if (hu.y == 0 && lane == 0) {
-          Fx g{0, 0};
-          init_row(a, a.cls.lo[0] + hu.x, r0, g);
-          a.hub_contrib[0][hu.x] = make_ulonglong2(0ull, g.dang);
-        }
-      } else {
-        const int G = 32 >> (c - 1);
-        const uint32_t r = a.cls.lo[c] + unit * (32u / G) + (uint32_t)(lane / G);
-        if (r < a.cls.hi[c] && lane % G == 0) init_row(a, r, r0, f);
-      }
-    }
+    for (uint64_t u = gtid; u < a.zi_lo; u += nthr) init_row(a, u, r0, f);
     sources_without_in_edges(a, r0, 0, f);
     const Fx b = block_sum_fx(f, sm.red);
-    if (threadIdx.x == 0) a.block_part[0][blockIdx.x] = make_ulonglong2(0ull, b.dang);
+    if (threadIdx.x == 0) a.block_part[0][blockIdx.x] = fx_pack(0, b.dang);
   }
   // rows without in-edges: next = base + d * 0 = base on every iteration
   // (1/n before the first), so their ranks follow in closed form; isolated
@@ -545,27 +935,59 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     // base = (1-d)/n + d*dangling_mass/n   (pagerank.rs:79)
     const double base = __dadd_rn(__ddiv_rn(1.0 - a.damping, nf),
                                   __ddiv_rn(__dmul_rn(a.damping, dm), nf));
-    if (threadIdx.x == 0) sm.next = 0;
-    load_hot(a, sm, cur);  // ends with a block barrier
+    // ---- phase A: every chunk of this block's range
+    if (threadIdx.x < kMaxGroups) sm.ctr[threadIdx.x] = 0;
+    __syncthreads();
     Fx f{0, 0};
-    // blocks own interleaved units (u = block + k * grid); warps of a block
-    // take kUnitsPerGrab of them at a time from the block's counter
-    for (bool done = false; !done;) {
-      uint32_t k = 0;
-      if (lane == 0) k = atomicAdd(&sm.next, (unsigned)kUnitsPerGrab);
-      k = __shfl_sync(0xffffffffu, k, 0);
-      for (uint32_t q = 0; q < (uint32_t)kUnitsPerGrab; q++) {
-        const uint32_t u = blockIdx.x + (k + q) * gridDim.x;
-        if (u >= a.n_units) {
-          done = true;
-          break;
-        }
-        run_unit<kW>(a, sm, u, cur, parity, base, f);
+    int loaded = -1;
+    const uint32_t n_sub = sm.n_sub;
+    for (uint32_t j = 0; j < n_sub; j++) {
+      const int sl = sm.sub_slice[j];
+      if (sl >= 0 && sl != loaded) {
+        __syncthreads();  // every warp is done with the previous slice
+        load_slice(a, sm, a.x[cur], sl, phase);
+        loaded = sl;
       }
+      const uint32_t cb = sm.sub_begin[j], ce = sm.sub_end[j];
+      for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(&sm.ctr[j], 1u);
+        k = __shfl_sync(0xffffffffu, k, 0) + cb;
+        if (k >= ce) break;
+        run_chunk<kW>(a, sm, k, cur, base, f);
+      }
+    }
+    grid_barrier(a.bar_count, a.bar_gen, gridDim.x, a.err, kWaitLimitNs);  // partials written
+    // ---- phase B: heavy rows combine their slots (slot order) and finish
+    for (uint32_t i = gwarp; i < a.n_wide; i += nwarps) {
+      const uint32_t r = a.wide_rows[i];
+      const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
+      F2 acc = f2_zero();
+      for (uint32_t k = s0 + lane; k < s1; k += 32) acc = f2_combine(acc, ldcg_f2(a.partial + k));
+      acc = warp_sum_f2(acc);
+      if (lane == 0)
+        finish_row(a, r, f2_value(acc), a.rank[cur][r], row_divisor(a, r), base, cur, f);
+    }
+    for (uint64_t r = gtid; r < a.H; r += nthr) {
+      const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
+      if (s1 - s0 > kWideSlots) continue;
+      const double old = a.rank[cur][r], div = row_divisor(a, r);
+      F2 acc = f2_zero();
+      uint32_t k = s0;
+      for (; k + 4 <= s1; k += 4) {
+        const F2 p0 = ldcg_f2(a.partial + k), p1 = ldcg_f2(a.partial + k + 1);
+        const F2 p2 = ldcg_f2(a.partial + k + 2), p3 = ldcg_f2(a.partial + k + 3);
+        acc = f2_combine(acc, p0);
+        acc = f2_combine(acc, p1);
+        acc = f2_combine(acc, p2);
+        acc = f2_combine(acc, p3);
+      }
+      for (; k < s1; k++) acc = f2_combine(acc, ldcg_f2(a.partial + k));
+      finish_row(a, r, f2_value(acc), old, div, base, cur, f);
     }
     sources_without_in_edges(a, base, cur ^ 1, f);
     const Fx b = block_sum_fx(f, sm.red);
-    if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = make_ulonglong2(b.delta, b.dang);
+    if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = fx_pack(b.delta, b.dang);
     tot = barrier_totals(a, parity, sm, Fin{n_zi * fabs(base - prev_iso), n_iso * base});
     prev_iso = base;
     delta = tot.delta;
@@ -575,9 +997,7 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
     if (delta < a.tol) break;  // every block sees the same delta
   }
   // rows without in-edges: the last iteration's base (1/n if none ran)
-  for (uint64_t u = a.zi_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.n;
-       u += (uint64_t)gridDim.x * kPrBlock)
-    a.rank[cur][u] = prev_iso;
+  for (uint64_t u = a.zi_lo + gtid; u < a.n; u += nthr) a.rank[cur][u] = prev_iso;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *a.out_iters = iters;
     *a.out_delta = delta;
@@ -587,7 +1007,7 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_persistent_k(PrArgs a) {
 
 // Weighted helpers: out-strength in out-CSR slot order (pagerank.rs:148-150,
 // the same sequential order, so the f64 sums are bit-identical), relabelled,
-// and the f32 weight of every execution-CSR slot.
+// and the f32 weight of every execution slot (0 for padding).
 __global__ void out_strength_new_k(const uint32_t* __restrict__ off,
                                    const uint32_t* __restrict__ eid, const double* __restrict__ w,
                                    const uint32_t* __restrict__ old_of_new, uint64_t n,
@@ -602,10 +1022,12 @@ __global__ void out_strength_new_k(const uint32_t* __restrict__ off,
 }
 
 __global__ void permute_w_f32_k(const uint32_t* __restrict__ eid, const double* __restrict__ w,
-                                uint64_t m, float* __restrict__ out) {
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-       k += (uint64_t)gridDim.x * blockDim.x)
-    out[k] = (float)w[eid[k]];
+                                uint64_t count, float* __restrict__ out) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t e = eid[k];
+    out[k] = e == kPadEid ? 0.f : (float)w[e];
+  }
 }
 
 __global__ void unpermute_k(const double* __restrict__ rank_new,
@@ -617,6 +1039,14 @@ __global__ void unpermute_k(const double* __restrict__ rank_new,
 }
 
 size_t pr_smem_bytes() { return sizeof(PrSmem); }
+
+template <class T>
+T read1(const T* d, cudaStream_t s) {
+  T h;
+  UG_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
 
 }  // namespace
 
@@ -634,68 +1064,163 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   }
   plan->new_of_old.alloc(n, s);
   plan->outdeg.alloc(n, s);
-  plan->off.alloc(n + 1, s);
-  Scratch<uint32_t> deg(n + 1, s);
+  Scratch<uint32_t> deg(n + 1, s), off(n + 1, s);
   relabel_maps_k<<<grid_for(n), kBlock, 0, s>>>(plan->old_of_new.get(), n, t->in.off.get(),
                                                  t->out.off.get(), plan->new_of_old.get(),
                                                  deg.get(), plan->outdeg.get());
   UG_LAUNCH_CHECK();
   UG_CUDA(cudaMemsetAsync(deg.get() + n, 0, sizeof(uint32_t), s));
-  exclusive_scan_u32(deg.get(), plan->off.get(), n + 1, nullptr, s);
-  plan->src.alloc(m ? m : 1, s);
-  plan->eid.alloc(m ? m : 1, s);
+  exclusive_scan_u32(deg.get(), off.get(), n + 1, nullptr, s);
+  Scratch<uint32_t> src(m ? m : 1, s), eid(m ? m : 1, s);
   if (m) {
-    relabel_copy_k<<<grid_for(m), kBlock, 0, s>>>(plan->off.get(), n, m, plan->old_of_new.get(),
+    relabel_copy_k<<<grid_for(m), kBlock, 0, s>>>(off.get(), n, m, plan->old_of_new.get(),
                                                    plan->new_of_old.get(), t->in.off.get(),
-                                                   t->in.tgt.get(), t->in.eid.get(),
-                                                   plan->src.get(), plan->eid.get());
+                                                   t->in.tgt.get(), t->in.eid.get(), src.get(),
+                                                   eid.get());
     UG_LAUNCH_CHECK();
   }
-  // ---- degree classes (rows are sorted by degree, so each is a range)
-  uint32_t bounds[kClasses + 1];
+  // ---- row classes
+  uint32_t bnd[3];
   {
-    Scratch<uint32_t> db(kClasses + 1, s);
-    class_bounds_k<<<1, 1, 0, s>>>(deg.get(), plan->outdeg.get(), n, db.get());
+    Scratch<uint32_t> d(3, s);
+    row_bounds_k<<<1, 1, 0, s>>>(deg.get(), plan->outdeg.get(), n, d.get());
     UG_LAUNCH_CHECK();
-    UG_CUDA(cudaMemcpyAsync(bounds, db.get(), sizeof(bounds), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaMemcpyAsync(bnd, d.get(), sizeof(bnd), cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));
   }
-  PrClassTable& c = plan->cls;
-  c.lo[0] = 0;
-  c.hi[0] = bounds[0];
-  for (int k = 1; k < kClasses; k++) {
-    c.lo[k] = bounds[k - 1];
-    c.hi[k] = k < kClasses - 1 ? bounds[k] : bounds[kClasses];  // up to the rows without in-edges
+  const uint32_t H = bnd[0];
+  plan->H = H;
+  plan->zi_lo = bnd[1];
+  plan->iso_lo = bnd[2];
+  UG_CHECK(H < (1u << 27), URSA_GPU_EINVAL, "pagerank: too many rows above the light-row degree");
+  // ---- heavy rows: per-segment counts and the number of 16-bit segments
+  uint32_t S = 0;
+  Scratch<uint32_t> cnt((uint64_t)(H ? H : 1) * kBins, s);
+  if (H) {
+    Scratch<unsigned long long> tot(2 * kBins, s);
+    UG_CUDA(cudaMemsetAsync(tot.get(), 0, 2 * kBins * sizeof(unsigned long long), s));
+    seg_hist_k<<<grid_for((uint64_t)H * 32), kBlock, 0, s>>>(off.get(), src.get(), H, cnt.get(),
+                                                             tot.get());
+    UG_LAUNCH_CHECK();
+    unsigned long long h[2 * kBins];
+    UG_CUDA(cudaMemcpyAsync(h, tot.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+    // a segment pays for its partial sums when its pieces average >= 3 edges
+    while (S < kSegMax && (uint64_t)S * kSegW < plan->iso_lo && h[kBins + S] > 0 &&
+           h[S] >= 3ull * h[kBins + S])
+      S++;
   }
-  plan->iso_lo = bounds[kClasses - 1];
-  plan->zi_lo = bounds[kClasses];
-  plan->n_hub = c.hi[0];
-  // hub chunks
-  plan->hub_nch.alloc(plan->n_hub ? plan->n_hub : 1, s);
-  plan->hub_first.alloc(plan->n_hub ? plan->n_hub : 1, s);
+  plan->S = S;
+  const uint32_t nb = S + 1;  // merged bins: segments 0..S-1, far
+  // ---- pieces and their slots (slot order: row, bin, piece)
+  Scratch<uint32_t> slot_base((uint64_t)(H ? H : 1) * nb, s);
+  uint32_t n_slots = 0;
+  plan->first_slot.alloc((uint64_t)H + 1, s);
+  if (H) {
+    Scratch<uint32_t> total(1, s);
+    piece_count_k<<<grid_for((uint64_t)H * nb), kBlock, 0, s>>>(cnt.get(), H, S, slot_base.get());
+    UG_LAUNCH_CHECK();
+    exclusive_scan_u32(slot_base.get(), slot_base.get(), (uint64_t)H * nb, total.get(), s);
+    first_slot_k<<<grid_for((uint64_t)H + 1), kBlock, 0, s>>>(slot_base.get(), H, S, total.get(),
+                                                              plan->first_slot.get());
+    UG_LAUNCH_CHECK();
+    n_slots = read1(total.get(), s);
+  } else {
+    UG_CUDA(cudaMemsetAsync(plan->first_slot.get(), 0, sizeof(uint32_t), s));
+  }
+  plan->n_slots = n_slots;
+  // ---- heavy rows' edges grouped by bin; pieces sorted by (bin, length desc)
+  const uint64_t m_heavy = H ? (uint64_t)read1(off.get() + H, s) : 0;
+  Scratch<uint32_t> segpre((uint64_t)(H ? H : 1) * nb, s);
+  Scratch<uint32_t> gsrc(m_heavy ? m_heavy : 1, s), geid(m_heavy ? m_heavy : 1, s);
+  Scratch<uint32_t> skey(n_slots ? n_slots : 1, s), order(n_slots ? n_slots : 1, s);
+  Scratch<uint32_t> prs(n_slots ? n_slots : 1, s);
+  uint32_t bb[kSegMax + 2] = {0};
+  if (H) {
+    group_rows_k<<<grid_for((uint64_t)H * 32), kBlock, 0, s>>>(off.get(), src.get(), eid.get(),
+                                                               cnt.get(), H, S, segpre.get(),
+                                                               gsrc.get(), geid.get());
+    UG_LAUNCH_CHECK();
+    Scratch<uint32_t> key(n_slots ? n_slots : 1, s);
+    piece_keys_k<<<grid_for((uint64_t)H * nb), kBlock, 0, s>>>(cnt.get(), slot_base.get(), H, S,
+                                                               key.get(), prs.get());
+    UG_LAUNCH_CHECK();
+    radix_sort_pairs(key.get(), nullptr, n_slots, bits_for(((uint64_t)S << 7) | 127u), skey.get(),
+                     order.get(), nullptr, nullptr, s);
+    Scratch<uint32_t> d(kSegMax + 2, s);
+    bin_bounds_k<<<1, 32, 0, s>>>(skey.get(), n_slots, S, d.get());
+    UG_LAUNCH_CHECK();
+    UG_CUDA(cudaMemcpyAsync(bb, d.get(), (S + 2) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+  }
+  // ---- chunk groups, in execution order: segments S-1..1, far, segment 0,
+  // light rows (segment 0 and the light rows share the segment-0 slice)
+  std::vector<GroupDesc> groups;
   uint32_t n_chunks = 0;
-  if (plan->n_hub) {
-    Scratch<uint32_t> tot(1, s);
-    hub_nch_k<<<grid_for(plan->n_hub), kBlock, 0, s>>>(deg.get(), plan->n_hub, plan->hub_nch.get());
-    UG_LAUNCH_CHECK();
-    exclusive_scan_u32(plan->hub_nch.get(), plan->hub_first.get(), plan->n_hub, tot.get(), s);
-    UG_CUDA(cudaMemcpyAsync(&n_chunks, tot.get(), 4, cudaMemcpyDeviceToHost, s));
-    UG_CUDA(cudaStreamSynchronize(s));
-  }
+  auto add_group = [&](int type, uint32_t bin, uint32_t ib, uint32_t ie, int slice) {
+    GroupDesc g{n_chunks, ib, ie, type, bin};
+    plan->group_begin[groups.size()] = n_chunks;
+    plan->group_slice[groups.size()] = slice;
+    groups.push_back(g);
+    n_chunks += (ie - ib + 31) / 32;
+  };
+  for (uint32_t b = S; b-- > 1;) add_group(0, b, bb[b], bb[b + 1], (int)b);
+  if (H) add_group(1, S, bb[S], bb[S + 1], -1);
+  if (S >= 1) add_group(0, 0, bb[0], bb[1], 0);
+  add_group(2, 0, H, plan->zi_lo, 0);
+  plan->n_groups = (uint32_t)groups.size();
+  plan->group_begin[groups.size()] = n_chunks;
   plan->n_chunks = n_chunks;
-  plan->hub_unit.alloc(n_chunks ? n_chunks : 1, s);
+  plan->chunks.alloc(n_chunks ? n_chunks : 1, s);
+  plan->chunk_slot.alloc((uint64_t)(n_chunks ? n_chunks : 1) * 32, s);
+  plan->cost_prefix.alloc((uint64_t)n_chunks + 1, s);
   if (n_chunks) {
-    hub_units_k<<<grid_for(plan->n_hub), kBlock, 0, s>>>(plan->hub_first.get(), plan->hub_nch.get(),
-                                                         plan->n_hub, plan->hub_unit.get());
+    Scratch<GroupDesc> dg(groups.size(), s);
+    UG_CUDA(cudaMemcpyAsync(dg.get(), groups.data(), groups.size() * sizeof(GroupDesc),
+                            cudaMemcpyHostToDevice, s));
+    Scratch<uint32_t> size16((uint64_t)n_chunks + 1, s), size32((uint64_t)n_chunks + 1, s);
+    Scratch<uint32_t> tot16(1, s), tot32(1, s);
+    UG_CUDA(cudaMemsetAsync(plan->cost_prefix.get() + n_chunks, 0, sizeof(uint32_t), s));
+    chunk_shape_k<<<grid_for(n_chunks), kBlock, 0, s>>>(dg.get(), (int)groups.size(), n_chunks,
+                                                        skey.get(), deg.get(), plan->chunks.get(),
+                                                        size16.get(), size32.get(),
+                                                        plan->cost_prefix.get());
     UG_LAUNCH_CHECK();
+    exclusive_scan_u32(size16.get(), size16.get(), n_chunks, tot16.get(), s);
+    exclusive_scan_u32(size32.get(), size32.get(), n_chunks, tot32.get(), s);
+    exclusive_scan_u32(plan->cost_prefix.get(), plan->cost_prefix.get(), (uint64_t)n_chunks + 1,
+                       nullptr, s);
+    chunk_base_k<<<grid_for(n_chunks), kBlock, 0, s>>>(n_chunks, size16.get(), size32.get(),
+                                                       plan->chunks.get());
+    UG_LAUNCH_CHECK();
+    const uint32_t n16 = read1(tot16.get(), s), n32 = read1(tot32.get(), s);
+    plan->n16 = n16;
+    plan->n32 = n32;
+    plan->ids16.alloc(n16 ? n16 : 8, s);
+    plan->eid16.alloc(n16 ? n16 : 8, s);
+    plan->ids32.alloc(n32 ? n32 : 4, s);
+    plan->eid32.alloc(n32 ? n32 : 4, s);
+    chunk_fill_k<<<grid_for((uint64_t)n_chunks * 32), kBlock, 0, s>>>(
+        dg.get(), (int)groups.size(), n_chunks, plan->chunks.get(), skey.get(), order.get(),
+        prs.get(), slot_base.get(), segpre.get(), gsrc.get(), geid.get(), off.get(), src.get(),
+        eid.get(), deg.get(), S, n, n_slots, plan->ids16.get(), plan->eid16.get(),
+        plan->ids32.get(), plan->eid32.get(), plan->chunk_slot.get());
+    UG_LAUNCH_CHECK();
+    UG_CUDA(cudaStreamSynchronize(s));  // dg's host source must outlive the copy
+  } else {
+    UG_CUDA(cudaMemsetAsync(plan->cost_prefix.get(), 0, sizeof(uint32_t), s));
   }
-  c.unit_begin[0] = 0;
-  c.unit_begin[1] = n_chunks;
-  for (int k = 1; k < kClasses; k++) {
-    const uint32_t G = 32u >> (k - 1), rpu = 32u / G;
-    c.unit_begin[k + 1] = c.unit_begin[k] + (c.hi[k] - c.lo[k] + rpu - 1) / rpu;
+  // ---- heavy rows combined by a warp in phase B
+  plan->wide_rows.alloc(H ? H : 1, s);
+  if (H) {
+    Scratch<uint32_t> flag(H, s), pos(H, s), tot(1, s);
+    wide_flag_k<<<grid_for(H), kBlock, 0, s>>>(plan->first_slot.get(), H, flag.get());
+    UG_LAUNCH_CHECK();
+    exclusive_scan_u32(flag.get(), pos.get(), H, tot.get(), s);
+    wide_scatter_k<<<grid_for(H), kBlock, 0, s>>>(flag.get(), pos.get(), H, plan->wide_rows.get());
+    UG_LAUNCH_CHECK();
+    plan->n_wide = read1(tot.get(), s);
   }
-  plan->n_units = c.unit_begin[kClasses];
   UG_CUDA(cudaStreamSynchronize(s));
   return plan;
 }
@@ -715,11 +1240,9 @@ static int pr_grid(int device) {
   if (device < 0 || device >= 64) device = 0;
   if (!cached[device]) {
     const int smem = (int)pr_smem_bytes();
-    UG_CUDA(cudaFuncSetAttribute(pr_persistent_k<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem));
+    UG_CUDA(cudaFuncSetAttribute(pr_seg_k<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
-    UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_persistent_k<kW>, kPrBlock,
-                                                          smem));
+    UG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_seg_k<kW>, kPrBlock, smem));
     UG_CHECK(per_sm > 0, URSA_GPU_ECUDA, "pagerank kernel cannot be resident");
     cached[device] = per_sm * sm_count(device);
   }
@@ -730,71 +1253,79 @@ static int pr_grid(int device) {
 // (device).  d_weights (device, by edge row) selects the weighted variant.
 void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* d_weights,
                   double* d_out, cudaStream_t s, ursa_gpu_pagerank_stats* stats) {
-  const uint64_t n = t->n, m = t->m;
+  const uint64_t n = t->n;
   if (stats) *stats = ursa_gpu_pagerank_stats{0, 0.0, 0.0};
   if (n == 0) return;
   PrPlan* plan = ensure_pr_plan(t, s);
   const bool weighted = d_weights != nullptr;
   const int G = weighted ? pr_grid<true>(t->device) : pr_grid<false>(t->device);
   const size_t smem = pr_smem_bytes();
-  const uint32_t nh = plan->n_hub ? plan->n_hub : 1;
 
   Scratch<double> rank(2 * n, s);
-  const uint64_t n_pad = (n + 3) & ~3ull;  // both share buffers 16-byte aligned
-  Scratch<float> x(2 * n_pad, s);
-  Scratch<F2> chunk_part(plan->n_chunks ? plan->n_chunks : 1, s);
-  Scratch<unsigned> hub_cnt(nh, s);
-  Scratch<ulonglong2> hub_contrib(2 * (size_t)nh, s);
-  Scratch<ulonglong2> block_part(2 * (size_t)G, s);
+  // share buffers: every slice [s*kSegW, +kSegW) a CTA may load, and the zero
+  // share of padding id n; entries beyond n stay zero
+  uint64_t cap = std::max<uint64_t>(n + 1, (uint64_t)std::max<uint32_t>(plan->S, 1u) * kSegW);
+  cap = (cap + 3) & ~3ull;
+  Scratch<float> x(2 * cap, s);
+  Scratch<F2> partial((uint64_t)plan->n_slots + 1, s);
+  Scratch<FxPair> block_part(2 * (size_t)G, s);
   Scratch<double2> totals(2, s);
   Scratch<unsigned> ctl(8, s);  // bar_count, bar_gen, err, iters, buf
   Scratch<double> ctl_d(1, s);
-  UG_CUDA(cudaMemsetAsync(hub_cnt.get(), 0, nh * sizeof(unsigned), s));
-  UG_CUDA(cudaMemsetAsync(hub_contrib.get(), 0, 2 * (size_t)nh * sizeof(ulonglong2), s));
+  UG_CUDA(cudaMemsetAsync(x.get(), 0, 2 * cap * sizeof(float), s));
   UG_CUDA(cudaMemsetAsync(ctl.get(), 0, 8 * sizeof(unsigned), s));
 
   Scratch<double> out_str;
-  Scratch<float> w_new;
+  Scratch<float> w16, w32;
   if (weighted) {
     out_str.alloc(n, s);
     out_strength_new_k<<<grid_for(n), kBlock, 0, s>>>(t->out.off.get(), t->out.eid.get(),
                                                        d_weights, plan->old_of_new.get(), n,
                                                        out_str.get());
     UG_LAUNCH_CHECK();
-    w_new.alloc(m ? m : 1, s);
-    if (m) {
-      permute_w_f32_k<<<grid_for(m), kBlock, 0, s>>>(plan->eid.get(), d_weights, m, w_new.get());
+    w16.alloc(plan->n16 ? plan->n16 : 8, s);
+    w32.alloc(plan->n32 ? plan->n32 : 4, s);
+    if (plan->n16) {
+      permute_w_f32_k<<<grid_for(plan->n16), kBlock, 0, s>>>(plan->eid16.get(), d_weights,
+                                                              plan->n16, w16.get());
+      UG_LAUNCH_CHECK();
+    }
+    if (plan->n32) {
+      permute_w_f32_k<<<grid_for(plan->n32), kBlock, 0, s>>>(plan->eid32.get(), d_weights,
+                                                              plan->n32, w32.get());
       UG_LAUNCH_CHECK();
     }
   }
 
   PrArgs a;
   a.n = n;
-  a.hot = (uint32_t)(n < (uint64_t)kHot ? n : (uint64_t)kHot);
-  a.cls = plan->cls;
-  a.n_units = plan->n_units;
-  a.off = plan->off.get();
-  a.src = plan->src.get();
-  a.w = weighted ? w_new.get() : nullptr;
+  a.H = plan->H;
+  a.zi_lo = plan->zi_lo;
+  a.iso_lo = plan->iso_lo;
+  a.n_chunks = plan->n_chunks;
+  a.n_groups = plan->n_groups;
+  a.n_wide = plan->n_wide;
+  for (int g = 0; g <= kMaxGroups; g++) a.group_begin[g] = plan->group_begin[g];
+  for (int g = 0; g < kMaxGroups; g++) a.group_slice[g] = plan->group_slice[g];
+  a.chunks = plan->chunks.get();
+  a.chunk_slot = plan->chunk_slot.get();
+  a.cost_prefix = plan->cost_prefix.get();
+  a.ids16 = plan->ids16.get();
+  a.ids32 = plan->ids32.get();
+  a.w16 = weighted ? w16.get() : nullptr;
+  a.w32 = weighted ? w32.get() : nullptr;
+  a.first_slot = plan->first_slot.get();
+  a.wide_rows = plan->wide_rows.get();
+  a.partial = partial.get();
   a.outdeg = plan->outdeg.get();
   a.out_str = weighted ? out_str.get() : nullptr;
   a.rank[0] = rank.get();
   a.rank[1] = rank.get() + n;
   a.x[0] = x.get();
-  a.x[1] = x.get() + n_pad;
-  a.hub_unit = plan->hub_unit.get();
-  a.hub_first = plan->hub_first.get();
-  a.hub_nch = plan->hub_nch.get();
-  a.n_hub = plan->n_hub;
-  a.chunk_part = chunk_part.get();
-  a.hub_cnt = hub_cnt.get();
-  a.hub_contrib[0] = hub_contrib.get();
-  a.hub_contrib[1] = hub_contrib.get() + nh;
+  a.x[1] = x.get() + cap;
   a.block_part[0] = block_part.get();
   a.block_part[1] = block_part.get() + G;
   a.totals = totals.get();
-  a.iso_lo = plan->iso_lo;
-  a.zi_lo = plan->zi_lo;
   a.bar_count = ctl.get() + 0;
   a.bar_gen = ctl.get() + 1;
   a.err = (int*)(ctl.get() + 2);
@@ -810,7 +1341,7 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   UG_CUDA(cudaEventCreate(&e1));
   UG_CUDA(cudaEventRecord(e0, s));
   void* args[] = {&a};
-  void* fn = weighted ? (void*)pr_persistent_k<true> : (void*)pr_persistent_k<false>;
+  void* fn = weighted ? (void*)pr_seg_k<true> : (void*)pr_seg_k<false>;
   UG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(kPrBlock), args, smem, s));
   count_launch();
   UG_CUDA(cudaEventRecord(e1, s));
@@ -823,7 +1354,7 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  UG_CHECK(h[2] == 0, URSA_GPU_ETIMEOUT, "pagerank: a grid barrier wait expired");
+  UG_CHECK(h[2] == 0, URSA_GPU_ETIMEOUT, "pagerank: a bounded wait in the kernel expired");
   const uint32_t buf = p.max_iter == 0 ? 0u : h[4];
   unpermute_k<<<grid_for(n), kBlock, 0, s>>>(rank.get() + (size_t)buf * n, plan->new_of_old.get(),
                                              n, d_out);
