@@ -63,6 +63,15 @@ int ursa_gpu_set_device(int device);
  * `device` enqueue their work: events recorded on it around a call give the
  * call's device time. */
 int ursa_gpu_thread_stream(int device, void **stream);
+/* Device memory: the library takes its device buffers (topologies, per-call
+ * scratch) from the device's stream-ordered memory pool and keeps every
+ * freed block cached in that pool, so repeated builds and calls never map
+ * memory from the driver again.  These report and return that cache (an
+ * extension with no counterpart in the reference): *cached = bytes the pool
+ * holds but no buffer uses; release returns all of them to the driver
+ * (other processes and allocators can then use the memory). */
+int ursa_gpu_pool_cached_bytes(int device, uint64_t *cached);
+int ursa_gpu_pool_release(int device);
 
 /* ---- Topology (ursa-core/src/topology.rs) ------------------------------ */
 
@@ -158,6 +167,17 @@ int ursa_gpu_bfs_distances_multi(ursa_gpu_topo *t, const uint32_t *sources, uint
 int ursa_gpu_shortest_path(ursa_gpu_topo *t, uint32_t source, uint32_t target, int dir,
                            uint32_t *path, uint64_t cap, int64_t *len);
 
+/* shortest_path over out-edges by the serving loop's algorithm, one query
+ * per launch: a bidirectional BFS in one CTA (forward on the out-CSR,
+ * backward on the in-CSR, the side with fewer frontier edges first; parents
+ * are the smallest-id discoverer on each level; the shortest meeting wins,
+ * ties to the smallest meeting id).  An extension with no counterpart in the
+ * reference: the path has the reference's hop count and is the path a
+ * server's shortest_path query returns, so it measures what batching adds to
+ * the same algorithm.  Paths longer than 4,096 nodes or cap: URSA_GPU_ETRUNC. */
+int ursa_gpu_shortest_path_bidirectional(ursa_gpu_topo *t, uint32_t source, uint32_t target,
+                                         uint32_t *path, uint64_t cap, int64_t *len);
+
 /* dijkstra_distances(&Topology, &[f64], u32, Direction) -> Vec<f64> --
  * algo/bfs.rs:126-166.  +inf = unreachable.  Distances are the same f64
  * values Dijkstra settles (min over paths of the left-to-right f64 sums). */
@@ -196,11 +216,16 @@ int ursa_gpu_connected_components_weak(ursa_gpu_topo *t, uint32_t *out);
  * that owns all device memory through its own pool.  The call allocates
  * nothing: the labels go to the caller's device array d_labels (n u32, same
  * minimum-member labels as the allocating form) and the union-find scratch
- * is a fixed array inside the library, 16 MiB per GPU, held by every GPU
- * that loads the library until the process exits.
+ * is a fixed array inside the library, 16 MiB per GPU.
  *  - Graphs above 4,194,304 nodes are rejected with URSA_GPU_EINVAL.
- *  - The first call on a device looks up that array's device address; make
- *    that first call before any stream capture.
+ *  - The first call on a device looks up that array's device address.  With
+ *    CUDA's default lazy module loading that first call is also when the
+ *    16 MiB array comes into being on that GPU (the driver loads the code
+ *    holding it), so make the first call on each GPU before free device
+ *    memory is handed out, and before any stream capture; the array then
+ *    stays until the process exits.
+ *  - Like every entry point here, the call makes the topology's device
+ *    current on the calling thread.
  *  - All calls on one GPU share the array: calls that overlap on the GPU
  *    (other threads, other streams) race and must be serialised by the caller.
  *  - stream: a cudaStream_t, or NULL for this thread's stream; the call
@@ -372,9 +397,10 @@ int ursa_gpu_batch_device_results(ursa_gpu_batch *b, const double **pagerank,
  *
  * The reference answers each query with one kernel call through its plan
  * layer: shortest_path (algo/bfs.rs:48-102, via ursa-plan/src/result.rs:216),
- * k_hop (algo/hop.rs:52-130, via result.rs:180) and pagerank
- * (algo/pagerank.rs:98-124, via result.rs:82-140).  A server keeps a resident
- * topology (shortest_path and hop queries) and uploaded small graphs
+ * k_hop (algo/hop.rs:52-130, via result.rs:180), bfs_distances
+ * (algo/bfs.rs:18-42) and pagerank (algo/pagerank.rs:98-124, via
+ * result.rs:82-140).  A server keeps a resident topology (shortest_path, hop
+ * and bfs queries) and uploaded small graphs
  * (pagerank queries) on the device and runs submitted queries with
  * continuous batching: each lane (a stream with preallocated slots, one
  * query type) launches one kernel for up to `slots` pending queries, lanes
@@ -385,14 +411,22 @@ int ursa_gpu_batch_device_results(ursa_gpu_batch *b, const double **pagerank,
  *    reference's serial-order choice), -1 length when there is none;
  *  - hop: the nodes k_hop(&[seed], k, Out) pairs with the seed, in the
  *    reference's emission order;
+ *  - bfs: bfs_distances(source, direction) -- n i32 hop distances, -1 where
+ *    unreached (all -1 for an out-of-range source); up to 64 queries of one
+ *    direction share a launch (one bit each in per-node masks);
  *  - pagerank: the batch kernel's ranks of the uploaded graph.
+ * Slot kernels wait for queries with bounded waits: they return when the
+ * scheduler's heartbeat (bumped every heartbeat_period_us) has not moved
+ * for heartbeat_limit_ns, and the server counts each such return in
+ * wait_expiries (the lane is relaunched for the next query).
  * ---------------------------------------------------------------------- */
 typedef struct ursa_gpu_server ursa_gpu_server;
 
 enum {
   URSA_GPU_QUERY_SHORTEST_PATH = 1,
   URSA_GPU_QUERY_HOP = 2,
-  URSA_GPU_QUERY_PAGERANK = 3
+  URSA_GPU_QUERY_PAGERANK = 3,
+  URSA_GPU_QUERY_BFS = 4
 };
 
 typedef struct {
@@ -402,6 +436,11 @@ typedef struct {
   uint64_t pr_max_nodes;           /* largest uploaded graph, in nodes */
   uint64_t hbm_reserve_bytes;      /* free HBM an upload must leave */
   uint64_t upload_budget_bytes;    /* device bytes of live uploads (0 = no cap) */
+  uint32_t bfs_lanes, bfs_slots;   /* bfs: lanes and queries per launch (<= 64) */
+  uint64_t heartbeat_limit_ns;     /* slot kernels return after this long without a
+                                      heartbeat (0 = 5 s) */
+  uint64_t heartbeat_period_us;    /* the scheduler bumps the heartbeat this often
+                                      (0 = every 1000 us) */
 } ursa_gpu_server_config;
 
 typedef struct {
@@ -411,12 +450,13 @@ typedef struct {
   uint32_t target;   /* shortest_path target */
   uint32_t k;        /* hop depth */
   ursa_gpu_pagerank_params pr;
+  uint32_t direction; /* bfs: 0 = Out, 1 = In, 2 = Both */
 } ursa_gpu_query;
 
 typedef struct {
   int32_t status;     /* URSA_GPU_OK, URSA_GPU_ECANCELED, ... */
   uint32_t type;
-  int64_t result_len; /* path nodes (-1 = no path), reached nodes, or ranks */
+  int64_t result_len; /* path nodes (-1 = no path), reached nodes, distances or ranks */
   uint32_t iterations;
   double last_delta;
   uint64_t edges;     /* edges the query scanned */
@@ -426,6 +466,7 @@ typedef struct {
 typedef struct {
   uint64_t submitted, completed, launches;
   uint64_t uploads_admitted, uploads_rejected, uploads_live, upload_bytes, pending;
+  uint64_t wait_expiries; /* slot kernels that returned because a bounded wait ran out */
 } ursa_gpu_server_stats;
 
 /* Creates a server over `resident` (may be NULL when no path/hop lanes are
@@ -456,8 +497,8 @@ int ursa_gpu_server_wait(ursa_gpu_server *s, uint64_t ticket, uint64_t timeout_u
 /* Tickets completed since the last poll (up to cap). */
 int ursa_gpu_server_poll(ursa_gpu_server *s, uint64_t *tickets, uint64_t cap, uint64_t *n_out);
 /* Hands over a completed query's result and forgets the ticket: u32 nodes
- * (path, hop) or f64 ranks (pagerank), info.result_len elements (0 for no
- * path); URSA_GPU_ETRUNC if cap_elems is too small. */
+ * (path, hop), i32 distances (bfs) or f64 ranks (pagerank), info.result_len
+ * elements (0 for no path); URSA_GPU_ETRUNC if cap_elems is too small. */
 int ursa_gpu_server_result(ursa_gpu_server *s, uint64_t ticket, ursa_gpu_query_info *info,
                            void *out, uint64_t cap_elems);
 int ursa_gpu_server_get_stats(ursa_gpu_server *s, ursa_gpu_server_stats *stats);

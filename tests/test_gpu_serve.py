@@ -5,12 +5,19 @@
     out-edges from source to target with the oracle's hop count;
   * hop: k_hop(&[seed], k) of the oracle and of the plain kernel, pair for
     pair in the reference's emission order (algo/hop.rs:52-130);
+  * bfs: bfs_distances(source, direction) of the oracle, exactly, in every
+    direction (ursa-core/src/algo/bfs.rs:18-42), out-of-range sources all -1;
   * pagerank on uploaded graphs: the oracle within the plain kernel's bounds
     (fixed iterations: max relative error <= 2e-6, L1 <= 1e-6);
+  * the one-query bidirectional shortest_path entry point returns exactly a
+    server's path (the same algorithm, no batching);
   * alone == in the mix: every query's result is bit-identical when it runs
     by itself and when it runs among hundreds of concurrent queries of all
     types;
-  * cancellation, upload admission by budget, release.
+  * cancellation, upload admission by budget, release;
+  * bounded waits: with the heartbeat stalled from the host, the slot
+    kernels give up after the configured limit, the server counts the
+    expiry, and the next query relaunches the lane.
 """
 
 import numpy as np
@@ -44,7 +51,7 @@ def _server(resident, **kw):
     from ursa_b200.serve import Server
 
     opts = dict(path_lanes=3, path_slots=8, hop_lanes=3, hop_slots=8, pr_lanes=2, pr_slots=16,
-                pr_max_nodes=1 << 16, hbm_reserve_bytes=1 << 30)
+                pr_max_nodes=1 << 16, hbm_reserve_bytes=1 << 30, bfs_lanes=2, bfs_slots=8)
     opts.update(kw)
     return Server(resident[3], **opts)
 
@@ -99,6 +106,68 @@ def test_hop_matches_plain_and_oracle(orc, resident, otopo):
                 assert np.array_equal(r.result, ref), (x, k)
 
 
+def test_bfs_vs_oracle(orc, resident, otopo):
+    from ursa_b200 import algo
+
+    n, _, _, topo = resident
+    rng = np.random.default_rng(17)
+    srcs = [int(x) for x in rng.integers(0, n, 40)] + [0, n - 42, n - 1, n + 7]
+    names = {0: "out", 1: "in", 2: "both"}
+    with _server(resident) as srv:
+        for d in (0, 1, 2):
+            tickets = [srv.bfs(x, d) for x in srcs]
+            for x, tk in zip(srcs, tickets):
+                r = srv.result(tk)
+                assert r.status == 0 and r.result.dtype == np.int32 and r.result.size == n
+                if x >= n:
+                    assert np.all(r.result == -1)
+                    continue
+                ref = orc.bfs_distances(otopo, x, names[d])
+                assert np.array_equal(r.result, ref), (x, d)
+                if d == 0 and x % 5 == 0:
+                    assert np.array_equal(r.result, algo.bfs_distances(topo, x, "out")), x
+
+
+def test_bidirectional_plain_call_equals_server_path(orc, resident, otopo):
+    from ursa_b200 import algo
+
+    n, _, _, topo = resident
+    off, tgt = otopo.csr("out")[:2]
+    qs = _path_queries(n, seed=11, count=60)
+    with _server(resident) as srv:
+        tickets = [srv.shortest_path(a, b) for a, b in qs]
+        for (a, b), tk in zip(qs, tickets):
+            r = srv.result(tk)
+            plain = algo.shortest_path_bidirectional(topo, a, b)
+            if r.result is None:
+                assert plain is None, (a, b)
+            else:
+                assert plain == [int(x) for x in r.result], (a, b)
+            _check_path(orc, otopo, (off, tgt), a, b, None if plain is None else np.array(plain, np.uint32))
+
+
+def test_heartbeat_expiry_is_counted_and_recovered(resident):
+    """The scheduler bumps the heartbeat only every 10 s here, and the slot
+    kernels wait at most 50 ms for a bump: they return on their own, the
+    server counts the expiry, and a later query relaunches the lane."""
+    import time
+
+    from ursa_b200 import algo
+
+    n, _, _, topo = resident
+    with _server(resident, path_lanes=1, path_slots=2, hop_lanes=1, hop_slots=2,
+                 heartbeat_limit_ns=50_000_000, heartbeat_period_us=10_000_000) as srv:
+        r = srv.result(srv.hop(3, 2))
+        assert r.status == 0
+        deadline = time.time() + 5.0
+        while srv.stats()["wait_expiries"] == 0 and time.time() < deadline:
+            time.sleep(0.05)
+        assert srv.stats()["wait_expiries"] >= 1
+        r2 = srv.result(srv.hop(5, 2))
+        assert r2.status == 0
+        assert np.array_equal(r2.result, algo.k_hop(topo, [5], 2)[1])
+
+
 def _uploads(count=12, seed=31):
     from ursa_b200 import gen
 
@@ -144,8 +213,10 @@ def test_alone_equals_in_mix(resident):
         mix = []
         for i in range(360):
             r = rng.random()
-            if r < 0.5:
+            if r < 0.42:
                 mix.append(("path", int(rng.integers(0, n)), int(rng.integers(0, n))))
+            elif r < 0.5:
+                mix.append(("bfs", int(rng.integers(0, n)), int(rng.integers(0, 3))))
             elif r < 0.8:
                 mix.append(("hop", int(rng.integers(0, n)), 2))
             else:
@@ -156,6 +227,8 @@ def test_alone_equals_in_mix(resident):
                 return srv.shortest_path(q[1], q[2])
             if q[0] == "hop":
                 return srv.hop(q[1], q[2])
+            if q[0] == "bfs":
+                return srv.bfs(q[1], q[2])
             return srv.pagerank(q[1], max_iter=100, tol=1e-7)
 
         alone = [srv.result(submit(q)) for q in mix]

@@ -67,7 +67,7 @@ class BatchConfig(C.Structure):
 
 BATCH_PAGERANK, BATCH_COMPONENTS, BATCH_TRIANGLES = 1, 2, 4
 
-QUERY_SHORTEST_PATH, QUERY_HOP, QUERY_PAGERANK = 1, 2, 3
+QUERY_SHORTEST_PATH, QUERY_HOP, QUERY_PAGERANK, QUERY_BFS = 1, 2, 3, 4
 
 
 class ServerConfig(C.Structure):
@@ -81,6 +81,10 @@ class ServerConfig(C.Structure):
         ("pr_max_nodes", C.c_uint64),
         ("hbm_reserve_bytes", C.c_uint64),
         ("upload_budget_bytes", C.c_uint64),
+        ("bfs_lanes", C.c_uint32),
+        ("bfs_slots", C.c_uint32),
+        ("heartbeat_limit_ns", C.c_uint64),
+        ("heartbeat_period_us", C.c_uint64),
     ]
 
 
@@ -92,6 +96,7 @@ class Query(C.Structure):
         ("target", C.c_uint32),
         ("k", C.c_uint32),
         ("pr", PageRankParams),
+        ("direction", C.c_uint32),
     ]
 
 
@@ -111,7 +116,8 @@ class QueryInfo(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "launches", "uploads_admitted",
-                                           "uploads_rejected", "uploads_live", "upload_bytes", "pending")]
+                                           "uploads_rejected", "uploads_live", "upload_bytes", "pending",
+                                           "wait_expiries")]
 
 # Every exported symbol with its (restype, argtypes).
 P, u32, u64, i32, i64, f64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_int64, C.c_double
@@ -141,6 +147,9 @@ SIGNATURES = {
     "ursa_gpu_bfs_distances": (i32, [P, u32, i32, P]),
     "ursa_gpu_bfs_distances_multi": (i32, [P, P, u64, i32, P]),
     "ursa_gpu_shortest_path": (i32, [P, u32, u32, i32, P, u64, C.POINTER(i64)]),
+    "ursa_gpu_pool_cached_bytes": (i32, [i32, C.POINTER(u64)]),
+    "ursa_gpu_pool_release": (i32, [i32]),
+    "ursa_gpu_shortest_path_bidirectional": (i32, [P, u32, u32, P, u64, C.POINTER(i64)]),
     "ursa_gpu_dijkstra_distances": (i32, [P, P, u64, u32, i32, P]),
     "ursa_gpu_shortest_path_weighted_with_cost": (
         i32,

@@ -102,6 +102,18 @@ def shortest_path(topo: Topology, source: int, target: int, direction=Direction.
     return None if ln.value < 0 else [int(x) for x in buf[: ln.value]]
 
 
+def shortest_path_bidirectional(topo: Topology, source: int, target: int):
+    """shortest_path over out-edges by the serving loop's bidirectional BFS,
+    one query per launch (an extension of algo/bfs.rs:48-102: same hop count,
+    ties resolved as a server's shortest_path query): node list or None."""
+    cap = 4096
+    buf = np.empty(cap, np.uint32)
+    ln = C.c_int64()
+    _lib.check(_lib.load().ursa_gpu_shortest_path_bidirectional(topo.handle, int(source), int(target),
+                                                                buf.ctypes.data, cap, C.byref(ln)))
+    return None if ln.value < 0 else [int(x) for x in buf[: ln.value]]
+
+
 def dijkstra_distances(topo: Topology, weights, source: int, direction=Direction.Out) -> np.ndarray:
     """dijkstra_distances (algo/bfs.rs:126-166)."""
     w = _f64(weights)

@@ -74,13 +74,25 @@ void prepare_device(int device) {
   UG_CHECK(device < cnt, URSA_GPU_ENODEV, "no such CUDA device");
   UG_CUDA(cudaSetDevice(device));
   UG_CUDA(cudaDeviceGetAttribute(&g_sm_count[device], cudaDevAttrMultiProcessorCount, device));
-  // Keep freed stream-ordered scratch in the pool instead of returning it to
-  // the driver after every call.
+  // Keep every freed stream-ordered block in the pool instead of returning it
+  // to the driver at the next synchronisation: a build whose transient
+  // scratch exceeded a finite threshold otherwise unmapped and re-mapped
+  // gigabytes on each call.  ursa_gpu_pool_release gives the cache back.
   cudaMemPool_t pool;
   UG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-  uint64_t threshold = 16ull << 30;  // keep up to 16 GiB of freed blocks for reuse
+  uint64_t threshold = UINT64_MAX;
   UG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
   g_prepared[device] = true;
+}
+
+uint64_t pool_cached_bytes(int device) {
+  prepare_device(device);
+  cudaMemPool_t pool;
+  UG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t reserved = 0, used = 0;  // the attributes are 64-bit
+  UG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+  UG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+  return reserved > used ? (uint64_t)(reserved - used) : 0;
 }
 
 int sm_count(int device) {
@@ -171,6 +183,24 @@ int ursa_gpu_set_device(int device) {
   return guard([&] {
     prepare_device(device);
     g_device = device;
+  });
+}
+
+int ursa_gpu_pool_cached_bytes(int device, uint64_t* cached) {
+  return guard([&] {
+    require(cached, "cached");
+    *cached = pool_cached_bytes(device);
+  });
+}
+
+int ursa_gpu_pool_release(int device) {
+  return guard([&] {
+    prepare_device(device);
+    cudaMemPool_t pool;
+    UG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    UG_CUDA(cudaSetDevice(device));
+    UG_CUDA(cudaDeviceSynchronize());  // frees still ordered on streams land in the pool first
+    UG_CUDA(cudaMemPoolTrimTo(pool, 0));
   });
 }
 

@@ -61,8 +61,9 @@ inline unsigned grid_for(uint64_t n, int block = kBlock, unsigned cap = 148u * 3
 }
 
 // Stream-ordered device scratch from the device's default memory pool. The
-// pool keeps freed blocks (release threshold raised once per device), so the
-// steady state allocates nothing from the driver.
+// pool keeps every freed block (its release threshold is raised to the
+// maximum once per device), so the steady state allocates nothing from the
+// driver.
 template <class T>
 struct Scratch {
   T* p = nullptr;
@@ -153,6 +154,9 @@ int guard(F&& f) {
 cudaStream_t thread_stream(int device);
 void prepare_device(int device);
 int sm_count(int device);
+// Bytes the device's memory pool holds that no buffer uses (free for the
+// library's next allocations, not for other allocators).
+uint64_t pool_cached_bytes(int device);
 
 // Device-side timeout for bounded waits (ns since an epoch).
 __device__ __forceinline__ uint64_t global_ns() {

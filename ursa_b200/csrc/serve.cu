@@ -24,6 +24,10 @@
 //  * hop: k_hop from one seed in the reference's exact emission order
 //    (level by level; within a level, candidates in the order of their
 //    parents and of the CSR, first occurrence kept, the seed excluded).
+//  * bfs: bfs_distances (algo/bfs.rs:18-42) for up to 64 queries of one
+//    direction per launch, bit q of per-node masks belonging to query q; one
+//    pull pass over the nodes per level (kernels that never wait on another
+//    CTA, so they share the GPU with the persistent slot kernels).
 //  * pagerank on uploaded graphs: the batch bucket kernel (batch.cu) over
 //    the launch's graphs, whose results do not depend on the other graphs.
 // Per-slot visit state is stamped (query base + level in the high word), so
@@ -375,6 +379,131 @@ __device__ HopOut hop_query(const HopArgs& A, const HopQuery q, const HopSlot& S
   return HopOut{pb - 1, status, scanned};
 }
 
+// One shortest_path query as its own launch (the plain form of a server
+// slot): the whole CTA runs path_query on fresh, zeroed visit arrays.
+__global__ void __launch_bounds__(kSvThreads) path_once_k(PathArgs A, PathQuery q, PathSlot S,
+                                                          uint32_t* path, PathOut* out,
+                                                          const uint32_t* cancel) {
+  __shared__ PathShared sh;
+  const PathOut o = path_query(A, q, S, path, cancel, sh);
+  if (threadIdx.x == 0) *out = o;
+}
+
+// --------------------------------------------------------------------- bfs
+// Level L of a batch: a node v still missing some queries ORs the frontier
+// masks of its pull neighbours (in-CSR for Out, out-CSR for In, undirected
+// CSR for Both) until every missing query has found it; the new bits become
+// v's next frontier mask and set its distance to L.  found[L & 1] records
+// whether the level reached anything; every kernel of level L first reads
+// found[(L + 1) & 1] (level L - 1) and returns at once when it is 0, so
+// levels enqueued past the end cost a launch each.  Nodes with more than
+// kBfsHub pull entries are done by a warp in bfs_level_hub_k.
+constexpr uint32_t kBfsHub = 64;
+
+struct BfsArgs {
+  const uint32_t* off;
+  const uint32_t* nbr;
+  uint64_t n;
+  const uint64_t* front;
+  uint64_t* next;
+  uint64_t* visited;
+  int32_t* dist;  // queries x n
+  uint64_t qmask;
+  int32_t level;
+  unsigned* found;  // [2]
+  const uint32_t* hubs;
+  uint32_t n_hubs;
+};
+
+__device__ __forceinline__ void bfs_settle(const BfsArgs& A, uint64_t v, uint64_t fresh) {
+  A.visited[v] |= fresh;
+  for (uint64_t bits = fresh; bits; bits &= bits - 1) {
+    const uint64_t q = (uint64_t)(__ffsll((long long)bits) - 1);
+    A.dist[q * A.n + v] = A.level;
+  }
+}
+
+__global__ void bfs_level_k(BfsArgs A) {
+  if (*(volatile unsigned*)&A.found[(A.level + 1) & 1] == 0) return;
+  bool any = false;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < A.n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t b = A.off[v], e = A.off[v + 1];
+    if (e - b > kBfsHub) continue;  // the hub kernel's
+    const uint64_t need = A.qmask & ~A.visited[v];
+    uint64_t fresh = 0;
+    if (need) {
+      uint64_t acc = 0;
+      for (uint32_t k = b; k < e; k++) {
+        acc |= A.front[A.nbr[k]];
+        if ((acc & need) == need) break;
+      }
+      fresh = acc & need;
+      if (fresh) {
+        bfs_settle(A, v, fresh);
+        any = true;
+      }
+    }
+    A.next[v] = fresh;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, any);  // every lane gets here
+  if (m && (threadIdx.x & 31) == __ffs(m) - 1) atomicOr(&A.found[A.level & 1], 1u);
+}
+
+__global__ void bfs_level_hub_k(BfsArgs A) {
+  if (*(volatile unsigned*)&A.found[(A.level + 1) & 1] == 0) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < A.n_hubs; i += nw) {
+    const uint32_t v = A.hubs[i];
+    const uint32_t b = A.off[v], e = A.off[v + 1];
+    const uint64_t need = A.qmask & ~A.visited[v];
+    uint64_t acc = 0;
+    for (uint32_t k0 = b; k0 < e && need; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      if (k < e) acc |= A.front[A.nbr[k]];
+      const uint64_t all = ((uint64_t)__reduce_or_sync(0xffffffffu, (unsigned)(acc >> 32)) << 32) |
+                           __reduce_or_sync(0xffffffffu, (unsigned)acc);
+      acc = all;
+      if ((acc & need) == need) break;
+    }
+    const uint64_t fresh = acc & need;
+    if (lane == 0) {
+      if (fresh) {
+        bfs_settle(A, v, fresh);
+        atomicOr(&A.found[A.level & 1], 1u);
+      }
+      A.next[v] = fresh;
+    }
+  }
+}
+
+// Sources of the batch: query q's bit at its source, distance 0.
+__global__ void bfs_seed_k(const uint32_t* __restrict__ src, uint32_t nq, uint64_t n,
+                           uint64_t* __restrict__ visited, uint64_t* __restrict__ front,
+                           int32_t* __restrict__ dist) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  const uint32_t s = src[q];
+  atomicOr((unsigned long long*)(visited + s), 1ull << q);
+  atomicOr((unsigned long long*)(front + s), 1ull << q);
+  dist[(uint64_t)q * n + s] = 0;
+}
+
+__global__ void bfs_hub_flag_k(const uint32_t* __restrict__ off, uint64_t n, uint32_t* __restrict__ flag) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    flag[v] = off[v + 1] - off[v] > kBfsHub ? 1u : 0u;
+}
+
+__global__ void bfs_hub_scatter_k(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                                  uint64_t n, uint32_t* __restrict__ hubs) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    if (flag[v]) hubs[pos[v]] = (uint32_t)v;
+}
+
 // ------------------------------------------------------- persistent lanes
 // A slot's query lives in DEVICE memory (the CTA polls only its own GPU's
 // memory): the host writes the fields with one async copy and then seq_in
@@ -411,6 +540,7 @@ struct LaneArgs {
   const HopSlot* hslots;
   uint64_t heartbeat_ns;  // return when the host's heartbeat stops this long
   uint64_t idle_ns;       // safety bound: return after this long without a query
+  uint32_t* expired;      // mapped host word: set when a bounded wait ran out
 };
 
 template <class T>
@@ -451,6 +581,8 @@ __global__ void __launch_bounds__(kSvThreads) lane_k(LaneArgs A) {
           t_hb = now;
         }
         if (now - t_hb > A.heartbeat_ns || now - t_idle > A.idle_ns) {
+          *(volatile uint32_t*)A.expired = 1u;  // the host counts the expiry
+          __threadfence_system();
           stop = 1;
           break;
         }
@@ -525,7 +657,7 @@ struct Request {
   std::shared_ptr<Upload> up;
 };
 
-enum LaneKind { kLanePath = 0, kLaneHop = 1, kLanePr = 2 };
+enum LaneKind { kLanePath = 0, kLaneHop = 1, kLanePr = 2, kLaneBfs = 3 };
 
 struct Lane {
   LaneKind kind;
@@ -545,6 +677,8 @@ struct Lane {
   HostMail* d_res = nullptr;      // device view
   uint32_t* paths = nullptr;      // mapped, host view
   uint32_t* d_paths = nullptr;
+  uint32_t* h_expired = nullptr;  // mapped word the slot kernels set on a wait expiry
+  uint32_t* d_expired = nullptr;
   std::vector<std::shared_ptr<Request>> slot_req;  // request in each slot (null = free)
   std::vector<uint32_t> seq;                       // last seq posted per slot
   std::vector<uint32_t> base;                      // next stamp base per slot
@@ -561,6 +695,17 @@ struct Lane {
   uint32_t* h_iters = nullptr;
   double* h_delta = nullptr;
   uint64_t pr_max_n = 0;
+  // bfs: one batch of up to 64 queries of one direction per launch
+  DevArray<uint64_t> b_vis, b_front[2];
+  DevArray<int32_t> b_dist;
+  DevArray<uint32_t> b_src;
+  DevArray<unsigned> b_found;
+  uint32_t* h_bsrc = nullptr;
+  unsigned* h_found = nullptr;
+  std::vector<int32_t> b_row;  // per queued request: its row in the batch, -1 = out of range
+  int32_t b_level = 0;         // last level enqueued
+  int b_dir = 0;
+  uint64_t b_qmask = 0;
 };
 
 }  // namespace
@@ -572,7 +717,11 @@ struct ursa_gpu_server {
   std::vector<std::unique_ptr<Lane>> lanes;
   std::mutex mu;
   std::condition_variable cv_sched, cv_done;
-  std::deque<std::shared_ptr<Request>> pending[3];
+  std::deque<std::shared_ptr<Request>> pending[4];
+  // pull-entry hubs of the resident topology per bfs direction (built on first use)
+  DevArray<uint32_t> bfs_hubs[3];
+  uint32_t bfs_n_hubs[3] = {0, 0, 0};
+  bool bfs_hubs_built[3] = {false, false, false};
   std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
   std::deque<uint64_t> completed;  // tickets not yet returned by poll
   std::unordered_map<uint32_t, std::shared_ptr<Upload>> uploads;
@@ -618,6 +767,9 @@ void lane_destroy(Lane& L) {
   free_pinned(L.paths);
   free_pinned(L.h_iters);
   free_pinned(L.h_delta);
+  free_pinned(L.h_expired);
+  free_pinned(L.h_bsrc);
+  free_pinned(L.h_found);
   if (L.done) cudaEventDestroy(L.done);
   if (L.stream) cudaStreamDestroy(L.stream);
   if (L.copy) cudaStreamDestroy(L.copy);
@@ -641,6 +793,7 @@ void lane_create(ursa_gpu_server* S, Lane& L, LaneKind kind, uint32_t slots) {
   UG_CUDA(cudaStreamCreateWithFlags(&L.copy, cudaStreamNonBlocking));
   UG_CUDA(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
   cudaStream_t s = L.stream;
+  L.h_expired = mapped_alloc<uint32_t>(1, &L.d_expired);
   if (kind == kLanePath || kind == kLaneHop) {
     L.d_mail.alloc(slots, s);
     UG_CUDA(cudaMemsetAsync(L.d_mail.get(), 0, slots * sizeof(DevMail), s));
@@ -689,6 +842,16 @@ void lane_create(ursa_gpu_server* S, Lane& L, LaneKind kind, uint32_t slots) {
     L.d_hslots.alloc(slots, s);
     UG_CUDA(cudaMemcpyAsync(L.d_hslots.get(), hs.data(), slots * sizeof(HopSlot),
                             cudaMemcpyHostToDevice, s));
+  } else if (kind == kLaneBfs) {
+    L.b_vis.alloc(nn, s);
+    L.b_front[0].alloc(nn, s);
+    L.b_front[1].alloc(nn, s);
+    L.b_dist.alloc((size_t)slots * nn, s);
+    L.b_src.alloc(slots, s);
+    L.b_found.alloc(2, s);
+    UG_CUDA(cudaMallocHost((void**)&L.h_bsrc, slots * 4));
+    UG_CUDA(cudaMallocHost((void**)&L.h_found, 2 * sizeof(unsigned)));
+    L.h_found[0] = L.h_found[1] = 0;
   } else {
     const uint64_t mx = S->cfg.pr_max_nodes;
     L.pr_max_n = mx;
@@ -722,8 +885,9 @@ void lane_start(ursa_gpu_server* S, Lane& L) {
   a.pslots = L.d_pslots.get();
   a.ha = HopArgs{t->out.off.get(), t->out.tgt.get(), t->n};
   a.hslots = L.d_hslots.get();
-  a.heartbeat_ns = kHeartbeatNs;
+  a.heartbeat_ns = S->cfg.heartbeat_limit_ns ? S->cfg.heartbeat_limit_ns : kHeartbeatNs;
   a.idle_ns = kIdleNs;
+  a.expired = L.d_expired;
   if (L.kind == kLanePath)
     lane_k<0><<<L.slots, kSvThreads, 0, L.stream>>>(a);
   else
@@ -858,6 +1022,145 @@ void pr_harvest(Lane& L) {
   UG_CUDA(cudaStreamSynchronize(L.copy));
 }
 
+// ---- bfs lanes
+struct PullCsr {
+  const uint32_t* off;
+  const uint32_t* nbr;
+};
+
+// Pull CSR of a bfs direction on the resident topology: Out pulls over the
+// in-CSR, In over the out-CSR, Both over the undirected CSR (built on first
+// use).
+PullCsr bfs_pull(ursa_gpu_server* S, int dir, cudaStream_t s) {
+  TopoImpl* t = S->topo;
+  if (dir == 2) {
+    ensure_undirected(t, s);
+    return PullCsr{t->und_off.get(), t->und_tgt.get()};
+  }
+  ensure_in(t, s);
+  if (dir == 1) return PullCsr{t->out.off.get(), t->out.tgt.get()};
+  return PullCsr{t->in.off.get(), t->in.tgt.get()};
+}
+
+// Nodes with more than kBfsHub pull entries, once per direction.
+void bfs_build_hubs(ursa_gpu_server* S, int dir, const PullCsr& c, cudaStream_t s) {
+  if (S->bfs_hubs_built[dir]) return;
+  const uint64_t n = S->topo->n;
+  Scratch<uint32_t> flag(n, s), pos(n, s), tot(1, s);
+  bfs_hub_flag_k<<<grid_for(n), kBlock, 0, s>>>(c.off, n, flag.get());
+  UG_LAUNCH_CHECK();
+  exclusive_scan_u32(flag.get(), pos.get(), n, tot.get(), s);
+  uint32_t nh = 0;
+  UG_CUDA(cudaMemcpyAsync(&nh, tot.get(), 4, cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaStreamSynchronize(s));
+  S->bfs_hubs[dir].alloc(nh ? nh : 1, s);
+  if (nh) {
+    bfs_hub_scatter_k<<<grid_for(n), kBlock, 0, s>>>(flag.get(), pos.get(), n, S->bfs_hubs[dir].get());
+    UG_LAUNCH_CHECK();
+  }
+  UG_CUDA(cudaStreamSynchronize(s));
+  S->bfs_n_hubs[dir] = nh;
+  S->bfs_hubs_built[dir] = true;
+}
+
+constexpr int32_t kBfsLevelsPerStep = 8;
+
+// Enqueues the batch's next kBfsLevelsPerStep levels, then the copy of the
+// last level's found flag into h_found[0] and the lane's event.
+void bfs_enqueue_levels(ursa_gpu_server* S, Lane& L) {
+  const uint64_t n = S->topo->n;
+  cudaStream_t s = L.stream;
+  const PullCsr c = bfs_pull(S, L.b_dir, s);
+  BfsArgs a;
+  a.off = c.off;
+  a.nbr = c.nbr;
+  a.n = n;
+  a.visited = L.b_vis.get();
+  a.dist = L.b_dist.get();
+  a.qmask = L.b_qmask;
+  a.found = L.b_found.get();
+  a.hubs = S->bfs_hubs[L.b_dir].get();
+  a.n_hubs = S->bfs_n_hubs[L.b_dir];
+  for (int k = 0; k < kBfsLevelsPerStep; k++) {
+    const int32_t lvl = ++L.b_level;
+    a.level = lvl;
+    a.front = L.b_front[(lvl + 1) & 1].get();
+    a.next = L.b_front[lvl & 1].get();
+    UG_CUDA(cudaMemsetAsync(L.b_found.get() + (lvl & 1), 0, sizeof(unsigned), s));
+    bfs_level_k<<<grid_for(n), kBlock, 0, s>>>(a);
+    UG_LAUNCH_CHECK();
+    if (a.n_hubs) {
+      bfs_level_hub_k<<<grid_for((uint64_t)a.n_hubs * 32), kBlock, 0, s>>>(a);
+      UG_LAUNCH_CHECK();
+    }
+  }
+  UG_CUDA(cudaMemcpyAsync(L.h_found, L.b_found.get() + (L.b_level & 1), sizeof(unsigned),
+                          cudaMemcpyDeviceToHost, s));
+  UG_CUDA(cudaEventRecord(L.done, s));
+}
+
+// Starts a bfs batch for the lane's queued requests (server lock held):
+// in-range sources get a row and a bit; the others answer all -1.
+void bfs_launch(ursa_gpu_server* S, Lane& L) {
+  const uint64_t n = S->topo->n;
+  cudaStream_t s = L.stream;
+  const double t = now_us();
+  uint32_t nq = 0;
+  L.b_row.assign(L.reqs.size(), -1);
+  for (size_t i = 0; i < L.reqs.size(); i++) {
+    L.reqs[i]->info.launch_us = t;
+    const uint32_t src = L.reqs[i]->q.source;
+    if (src < n) {  // bfs.rs:21-23: an out-of-range source reaches nothing
+      L.h_bsrc[nq] = src;
+      L.b_row[i] = (int32_t)nq;
+      nq++;
+    }
+  }
+  L.b_dir = (int)L.reqs[0]->q.direction;
+  L.b_level = 0;
+  L.b_qmask = nq >= 64 ? ~0ull : ((1ull << nq) - 1ull);
+  L.running = true;
+  S->stats.launches++;
+  if (nq == 0) {
+    L.h_found[0] = 0;
+    UG_CUDA(cudaEventRecord(L.done, s));
+    return;
+  }
+  const PullCsr c = bfs_pull(S, L.b_dir, s);
+  bfs_build_hubs(S, L.b_dir, c, s);
+  UG_CUDA(cudaMemcpyAsync(L.b_src.get(), L.h_bsrc, nq * 4, cudaMemcpyHostToDevice, s));
+  UG_CUDA(cudaMemsetAsync(L.b_vis.get(), 0, n * 8, s));
+  UG_CUDA(cudaMemsetAsync(L.b_front[0].get(), 0, n * 8, s));
+  UG_CUDA(cudaMemsetAsync(L.b_dist.get(), 0xFF, (size_t)nq * n * 4, s));
+  UG_CUDA(cudaMemsetAsync(L.b_found.get(), 0x01, sizeof(unsigned), s));  // level 0 reached the sources
+  UG_CUDA(cudaMemsetAsync(L.b_found.get() + 1, 0, sizeof(unsigned), s));
+  bfs_seed_k<<<(nq + 63) / 64, 64, 0, s>>>(L.b_src.get(), nq, n, L.b_vis.get(), L.b_front[0].get(),
+                                           L.b_dist.get());
+  UG_LAUNCH_CHECK();
+  bfs_enqueue_levels(S, L);
+}
+
+// Copies each query's distance row out (the server lock is not held).
+void bfs_harvest(ursa_gpu_server* S, Lane& L) {
+  const uint64_t n = S->topo->n;
+  for (size_t i = 0; i < L.reqs.size(); i++) {
+    Request& r = *L.reqs[i];
+    r.info.status = URSA_GPU_OK;
+    r.info.result_len = (int64_t)n;
+    r.info.iterations = (uint32_t)L.b_level;
+    r.u32.resize(n);
+    const int32_t row = L.b_row[i];
+    if (row < 0) {
+      std::fill(r.u32.begin(), r.u32.end(), 0xFFFFFFFFu);
+      continue;
+    }
+    if (n)
+      UG_CUDA(cudaMemcpyAsync(r.u32.data(), L.b_dist.get() + (size_t)row * n, n * 4,
+                              cudaMemcpyDeviceToHost, L.copy));
+  }
+  UG_CUDA(cudaStreamSynchronize(L.copy));
+}
+
 void complete(ursa_gpu_server* S, const std::shared_ptr<Request>& r, double t) {
   r->info.done_us = t;
   r->done = true;
@@ -876,7 +1179,8 @@ void sched_loop(ursa_gpu_server* S) {
     bool progressed = false;
     try {
       const double t_now = now_us();
-      if (t_now - S->last_heartbeat > 1000.0) {  // about once a millisecond
+      const double period = S->cfg.heartbeat_period_us ? (double)S->cfg.heartbeat_period_us : 1000.0;
+      if (t_now - S->last_heartbeat > period) {  // about once a millisecond by default
         S->last_heartbeat = t_now;
         for (auto& lp : S->lanes)
           if (lp->h_ctl && lp->running) {
@@ -918,11 +1222,47 @@ void sched_loop(ursa_gpu_server* S) {
           }
           continue;
         }
+        if (L.kind == kLaneBfs) {
+          // bfs: more levels, or harvest a finished batch; then refill
+          if (L.running) {
+            const cudaError_t e = cudaEventQuery(L.done);
+            if (e == cudaErrorNotReady) continue;
+            UG_CUDA(e);
+            if (*(volatile unsigned*)L.h_found) {
+              bfs_enqueue_levels(S, L);
+              continue;
+            }
+            lk.unlock();
+            bfs_harvest(S, L);
+            lk.lock();
+            const double t = now_us();
+            for (auto& r : L.reqs) complete(S, r, t);
+            L.reqs.clear();
+            L.running = false;
+            progressed = true;
+          }
+          auto& bq = S->pending[kLaneBfs];
+          while (!bq.empty() && L.reqs.size() < L.slots) {
+            auto r = bq.front();
+            if (!L.reqs.empty() && r->q.direction != L.reqs[0]->q.direction) break;  // next launch
+            bq.pop_front();
+            L.reqs.push_back(r);
+          }
+          if (!L.reqs.empty()) {
+            bfs_launch(S, L);
+            progressed = true;
+          }
+          continue;
+        }
         // path / hop: finished slots out, pending queries into free slots
         if (L.running) {
           const cudaError_t e = cudaEventQuery(L.done);
           if (e == cudaSuccess) {
             L.running = false;  // every CTA returned
+            if (*(volatile uint32_t*)L.h_expired) {  // ... because a bounded wait ran out
+              *(volatile uint32_t*)L.h_expired = 0u;
+              S->stats.wait_expiries++;
+            }
           } else if (e != cudaErrorNotReady) {
             UG_CUDA(e);
           }
@@ -972,7 +1312,7 @@ void sched_loop(ursa_gpu_server* S) {
     if (!progressed) {
       bool any_busy = false;
       for (auto& lp : S->lanes) {
-        any_busy |= lp->running && lp->kind == kLanePr;
+        any_busy |= lp->running && (lp->kind == kLanePr || lp->kind == kLaneBfs);
         for (auto& r : lp->slot_req) any_busy |= r != nullptr;
       }
       if (any_busy) {
@@ -996,10 +1336,12 @@ int ursa_gpu_server_create(ursa_gpu_topo* resident, const ursa_gpu_server_config
   return guard([&] {
     UG_CHECK(out && cfg, URSA_GPU_EINVAL, "out / config is NULL");
     *out = nullptr;
-    UG_CHECK(cfg->path_lanes + cfg->hop_lanes + cfg->pr_lanes > 0, URSA_GPU_EINVAL,
+    UG_CHECK(cfg->path_lanes + cfg->hop_lanes + cfg->pr_lanes + cfg->bfs_lanes > 0, URSA_GPU_EINVAL,
              "server: no lanes configured");
-    UG_CHECK(!(cfg->path_lanes || cfg->hop_lanes) || resident, URSA_GPU_EINVAL,
-             "server: path and hop lanes need a resident topology");
+    UG_CHECK(!(cfg->path_lanes || cfg->hop_lanes || cfg->bfs_lanes) || resident, URSA_GPU_EINVAL,
+             "server: path, hop and bfs lanes need a resident topology");
+    UG_CHECK(cfg->bfs_lanes == 0 || (cfg->bfs_slots >= 1 && cfg->bfs_slots <= 64), URSA_GPU_EINVAL,
+             "server: bfs lanes need 1..64 slots");
     for (uint32_t v : {cfg->path_slots, cfg->hop_slots, cfg->pr_slots})
       UG_CHECK(v <= 1024, URSA_GPU_EINVAL, "server: at most 1024 slots per lane");
     UG_CHECK((cfg->path_lanes == 0 || cfg->path_slots) && (cfg->hop_lanes == 0 || cfg->hop_slots),
@@ -1040,6 +1382,7 @@ int ursa_gpu_server_create(ursa_gpu_topo* resident, const ursa_gpu_server_config
       add(kLanePath, cfg->path_lanes, cfg->path_slots);
       add(kLaneHop, cfg->hop_lanes, cfg->hop_slots);
       add(kLanePr, cfg->pr_lanes, cfg->pr_slots);
+      add(kLaneBfs, cfg->bfs_lanes, cfg->bfs_slots);
     } catch (...) {
       for (auto& l : S->lanes) lane_raise_stop(*l);
       for (auto& l : S->lanes) lane_destroy(*l);
@@ -1079,6 +1422,7 @@ int ursa_gpu_server_upload(ursa_gpu_server* S, uint64_t n_nodes, const uint32_t*
     size_t free_b = 0, total_b = 0;
     UG_CUDA(cudaSetDevice(S->device));
     UG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    free_b += pool_cached_bytes(S->device);  // blocks the pool keeps are free for the build
     {
       std::lock_guard<std::mutex> g(S->mu);
       const bool fits = free_b > S->cfg.hbm_reserve_bytes && free_b - S->cfg.hbm_reserve_bytes >= need &&
@@ -1148,6 +1492,11 @@ int ursa_gpu_server_submit(ursa_gpu_server* S, const ursa_gpu_query* q, uint64_t
       case URSA_GPU_QUERY_HOP:
         UG_CHECK(S->cfg.hop_lanes, URSA_GPU_EINVAL, "server has no hop lanes");
         kind = kLaneHop;
+        break;
+      case URSA_GPU_QUERY_BFS:
+        UG_CHECK(S->cfg.bfs_lanes, URSA_GPU_EINVAL, "server has no bfs lanes");
+        UG_CHECK(q->direction <= 2, URSA_GPU_EINVAL, "bfs query: direction must be 0, 1 or 2");
+        kind = kLaneBfs;
         break;
       case URSA_GPU_QUERY_PAGERANK: {
         UG_CHECK(S->cfg.pr_lanes, URSA_GPU_EINVAL, "server has no pagerank lanes");
@@ -1259,6 +1608,45 @@ int ursa_gpu_server_result(ursa_gpu_server* S, uint64_t ticket, ursa_gpu_query_i
         std::memcpy(out, r->u32.data(), len * 4);
     }
     S->reqs.erase(it);  // the result is handed over once
+  });
+}
+
+int ursa_gpu_shortest_path_bidirectional(ursa_gpu_topo* t, uint32_t source, uint32_t target,
+                                         uint32_t* path, uint64_t cap, int64_t* len) {
+  return guard([&] {
+    UG_CHECK(t && len, URSA_GPU_EINVAL, "topology / len is NULL");
+    TopoImpl* ti = &t->impl;
+    cudaStream_t s = thread_stream(ti->device);
+    ensure_in(ti, s);
+    const uint64_t n = ti->n, nn = n ? n : 1;
+    Scratch<uint64_t> fpar(nn, s), bpar(nn, s);
+    Scratch<uint32_t> q0(nn, s), q1(nn, s), q2(nn, s), q3(nn, s), d_path(kPathCap, s), cancel(1, s);
+    Scratch<PathOut> d_out(1, s);
+    UG_CUDA(cudaMemsetAsync(fpar.get(), 0, nn * 8, s));
+    UG_CUDA(cudaMemsetAsync(bpar.get(), 0, nn * 8, s));
+    UG_CUDA(cudaMemsetAsync(cancel.get(), 0, 4, s));
+    PathSlot ps;
+    ps.fpar = fpar.get();
+    ps.bpar = bpar.get();
+    ps.q[0] = q0.get();
+    ps.q[1] = q1.get();
+    ps.q[2] = q2.get();
+    ps.q[3] = q3.get();
+    const PathArgs pa{ti->out.off.get(), ti->out.tgt.get(), ti->in.off.get(), ti->in.tgt.get(), n};
+    path_once_k<<<1, kSvThreads, 0, s>>>(pa, PathQuery{source, target, kStampStride}, ps, d_path.get(),
+                                         d_out.get(), cancel.get());
+    UG_LAUNCH_CHECK();
+    PathOut o;
+    UG_CUDA(cudaMemcpyAsync(&o, d_out.get(), sizeof(o), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+    *len = o.len;
+    UG_CHECK(o.status == URSA_GPU_OK, o.status, "shortest_path_bidirectional: path too long");
+    if (o.len > 0) {
+      UG_CHECK((uint64_t)o.len <= cap, URSA_GPU_ETRUNC, "shortest_path_bidirectional: path longer than cap");
+      UG_CHECK(path, URSA_GPU_EINVAL, "path is NULL");
+      UG_CUDA(cudaMemcpyAsync(path, d_path.get(), (size_t)o.len * 4, cudaMemcpyDeviceToHost, s));
+      UG_CUDA(cudaStreamSynchronize(s));
+    }
   });
 }
 

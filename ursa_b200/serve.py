@@ -1,10 +1,11 @@
 """The serving loop (the ursa_gpu_server_* entry points of include/ursa_gpu.h).
 
-A Server keeps a resident Topology (shortest_path and hop queries) and
+A Server keeps a resident Topology (shortest_path, hop and bfs queries) and
 uploaded small graphs (pagerank queries) on the device and runs submitted
 queries with continuous batching.  Query meanings follow the reference's
 kernels: shortest_path (ursa-core/src/algo/bfs.rs:48-102), k_hop from one
-seed (algo/hop.rs:52-130) and pagerank (algo/pagerank.rs:98-124).
+seed (algo/hop.rs:52-130), bfs_distances (algo/bfs.rs:18-42) and pagerank
+(algo/pagerank.rs:98-124).
 """
 
 from __future__ import annotations
@@ -17,9 +18,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import QUERY_HOP, QUERY_PAGERANK, QUERY_SHORTEST_PATH, PageRankParams, Query, QueryInfo, ServerConfig
+from ._lib import (QUERY_BFS, QUERY_HOP, QUERY_PAGERANK, QUERY_SHORTEST_PATH, PageRankParams, Query, QueryInfo,
+                   ServerConfig)
 
-__all__ = ["Server", "Completed", "QUERY_SHORTEST_PATH", "QUERY_HOP", "QUERY_PAGERANK"]
+__all__ = ["Server", "Completed", "QUERY_SHORTEST_PATH", "QUERY_HOP", "QUERY_PAGERANK", "QUERY_BFS"]
 
 # Servers still open at interpreter exit are closed before the CUDA runtime
 # shuts down (a server's scheduler thread and resident kernels must not
@@ -41,7 +43,7 @@ class Completed:
     ticket: int
     status: int
     type: int
-    result: np.ndarray | None  # path / reached nodes (u32) or ranks (f64); None: no path
+    result: np.ndarray | None  # path / reached nodes (u32), distances (i32) or ranks (f64); None: no path
     iterations: int
     last_delta: float
     edges: int
@@ -56,9 +58,11 @@ class Completed:
 
 class Server:
     def __init__(self, resident=None, *, path_lanes=4, path_slots=8, hop_lanes=4, hop_slots=8, pr_lanes=2,
-                 pr_slots=32, pr_max_nodes=65536, hbm_reserve_bytes=8 << 30, upload_budget_bytes=0):
+                 pr_slots=32, pr_max_nodes=65536, hbm_reserve_bytes=8 << 30, upload_budget_bytes=0,
+                 bfs_lanes=0, bfs_slots=16, heartbeat_limit_ns=0, heartbeat_period_us=0):
         cfg = ServerConfig(path_lanes, path_slots, hop_lanes, hop_slots, pr_lanes, pr_slots, pr_max_nodes,
-                           hbm_reserve_bytes, upload_budget_bytes)
+                           hbm_reserve_bytes, upload_budget_bytes, bfs_lanes, bfs_slots, heartbeat_limit_ns,
+                           heartbeat_period_us)
         h = C.c_void_p()
         self._resident = resident  # kept alive for the server's lifetime
         _lib.check(_lib.load().ursa_gpu_server_create(resident.handle if resident is not None else None,
@@ -116,6 +120,10 @@ class Server:
     def pagerank(self, graph_id: int, damping=0.85, max_iter=30, tol=1e-6) -> int:
         return self._submit(Query(QUERY_PAGERANK, graph_id, 0, 0, 0, PageRankParams(damping, max_iter, tol)))
 
+    def bfs(self, source: int, direction: int = 0) -> int:
+        """bfs_distances(source, direction): 0 = Out, 1 = In, 2 = Both."""
+        return self._submit(Query(QUERY_BFS, 0, source, 0, 0, PageRankParams(0.85, 30, 1e-6), direction))
+
     def cancel(self, ticket: int) -> None:
         _lib.check(_lib.load().ursa_gpu_server_cancel(self.handle, ticket))
 
@@ -137,6 +145,8 @@ class Server:
         n = max(int(info.result_len), 0)
         if info.type == QUERY_PAGERANK:
             out = np.empty(n, np.float64)
+        elif info.type == QUERY_BFS:
+            out = np.empty(n, np.int32)
         else:
             out = np.empty(n, np.uint32)
         _lib.check(L.ursa_gpu_server_result(self.handle, ticket, C.byref(info), out.ctypes.data if n else None, n))
