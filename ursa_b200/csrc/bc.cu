@@ -23,6 +23,7 @@
 // order, and sampled results are scaled by n / k (accumulate_sources,
 // :45-70; :171-176).  The dependency sums run in a different order than the
 // reference's predecessor lists, so results agree to f64 rounding.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -219,7 +220,247 @@ __global__ void fdeg_out_k(const uint32_t* __restrict__ off, const uint32_t* __r
     pos[i] = i < f ? (uint64_t)(off[F[i] + 1] - off[F[i]]) : 0ull;
 }
 
+// ---- 64 sources at once (unweighted) -------------------------------------
+// Batch b holds sources [64 b, 64 b + 64) of the source list, the
+// reference's accumulation chunk (betweenness.rs:45-70).  Per node v the
+// batch keeps a row of 64 values per quantity (hop i32, sigma f64, delta
+// f64; node-major, so lane j of a warp reads entries j and j + 32 of a row
+// in one coalesced access), a visited mask and a frontier mask (bit q =
+// source q).
+//  forward level L: one warp per node v still missing some sources; it walks
+//    v's in-edges u -> v in CSR order (eight in flight); the sources in
+//    front[u] & need reach v at level L, sigma_q[v] += sigma_q[u] for each
+//    (per slot, as brandes_from counts parallel edges), and the slot of the
+//    out-CSR holding u -> v records those sources (dag[], the shortest-path
+//    DAG per source);
+//  backward level L (deepest first): one warp per node v with some source at
+//    level L; over v's out-edges in CSR order, for each source q of dag[k]
+//    at level L, delta_q[v] += sigma_q[v] * ((1 + delta_q[w]) / sigma_q[w])
+//    (reverse_accumulate, :81-98, summed per successor instead of per
+//    predecessor list);
+//  fold: per node, the batch's partial = sum over q in source order of
+//    delta_q[v] (v != source q), added to the result in batch order.
+constexpr int kBcB = 64;
+
+struct BcBatchArgs {
+  const uint32_t* in_off;
+  const uint32_t* in_src;
+  const uint32_t* in_to_out;  // in-CSR slot -> out-CSR slot of the same edge
+  const uint32_t* out_off;
+  const uint32_t* out_tgt;
+  uint64_t n;
+  uint64_t qmask;
+  uint64_t* vis;
+  const uint64_t* front;
+  uint64_t* next;
+  int32_t* hop;      // n x 64
+  double* sigma;     // n x 64
+  double* delta;     // n x 64
+  uint64_t* dag;     // per out-CSR slot
+  int32_t level;
+  unsigned* found;
+};
+
+__global__ void bc_seed_k(const uint32_t* __restrict__ src, uint32_t nq, uint64_t* vis, uint64_t* front,
+                          int32_t* hop, double* sigma) {
+  const uint32_t q = threadIdx.x;
+  if (q >= nq) return;
+  const uint32_t s = src[q];
+  atomicOr((unsigned long long*)(vis + s), 1ull << q);
+  atomicOr((unsigned long long*)(front + s), 1ull << q);
+  hop[(uint64_t)s * kBcB + q] = 0;
+  sigma[(uint64_t)s * kBcB + q] = 1.0;
+}
+
+__global__ void bc_forward_k(BcBatchArgs A) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  bool any = false;
+  for (uint64_t v = gw; v < A.n; v += nw) {
+    const uint64_t need = A.qmask & ~A.vis[v];
+    if (need == 0) {
+      if (lane == 0) A.next[v] = 0;
+      continue;
+    }
+    const uint32_t b = A.in_off[v], e = A.in_off[v + 1];
+    double s0 = 0.0, s1 = 0.0;
+    uint64_t reached = 0;
+    for (uint32_t k0 = b; k0 < e; k0 += 8) {
+      uint32_t u = 0;
+      uint64_t f = 0;
+      if (lane < 8 && k0 + lane < e) {
+        u = A.in_src[k0 + lane];
+        f = A.front[u] & need;
+        if (f) A.dag[A.in_to_out[k0 + lane]] = f;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t fj = __shfl_sync(0xffffffffu, f, j);
+        const uint32_t uj = __shfl_sync(0xffffffffu, u, j);
+        if (fj) {
+          reached |= fj;
+          const double* row = A.sigma + (uint64_t)uj * kBcB;
+          if ((fj >> lane) & 1ull) s0 += row[lane];
+          if ((fj >> (lane + 32)) & 1ull) s1 += row[lane + 32];
+        }
+      }
+    }
+    if (lane == 0) A.next[v] = reached;
+    if (reached) {
+      any = true;
+      if (lane == 0) A.vis[v] |= reached;
+      if ((reached >> lane) & 1ull) {
+        A.sigma[v * kBcB + lane] = s0;
+        A.hop[v * kBcB + lane] = A.level;
+      }
+      if ((reached >> (lane + 32)) & 1ull) {
+        A.sigma[v * kBcB + lane + 32] = s1;
+        A.hop[v * kBcB + lane + 32] = A.level;
+      }
+    }
+  }
+  if (lane == 0 && any) atomicOr(A.found, 1u);
+}
+
+__global__ void bc_backward_k(BcBatchArgs A) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = gw; v < A.n; v += nw) {
+    const bool h0 = A.hop[v * kBcB + lane] == A.level;
+    const bool h1 = A.hop[v * kBcB + lane + 32] == A.level;
+    const uint64_t mL = (uint64_t)__ballot_sync(0xffffffffu, h0) |
+                        ((uint64_t)__ballot_sync(0xffffffffu, h1) << 32);
+    if (mL == 0) continue;
+    const double sv0 = h0 ? A.sigma[v * kBcB + lane] : 0.0;
+    const double sv1 = h1 ? A.sigma[v * kBcB + lane + 32] : 0.0;
+    double d0 = 0.0, d1 = 0.0;
+    const uint32_t b = A.out_off[v], e = A.out_off[v + 1];
+    for (uint32_t k0 = b; k0 < e; k0 += 8) {
+      uint32_t w = 0;
+      uint64_t dm = 0;
+      if (lane < 8 && k0 + lane < e) {
+        dm = A.dag[k0 + lane] & mL;
+        if (dm) w = A.out_tgt[k0 + lane];
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t dj = __shfl_sync(0xffffffffu, dm, j);
+        const uint32_t wj = __shfl_sync(0xffffffffu, w, j);
+        if (dj) {
+          const uint64_t r = (uint64_t)wj * kBcB;
+          if ((dj >> lane) & 1ull)  // coeff = (1 + delta[w]) / sigma[w]; delta[v] += sigma[v] * coeff
+            d0 += __dmul_rn(sv0, __ddiv_rn(__dadd_rn(1.0, A.delta[r + lane]), A.sigma[r + lane]));
+          if ((dj >> (lane + 32)) & 1ull)
+            d1 += __dmul_rn(sv1, __ddiv_rn(__dadd_rn(1.0, A.delta[r + lane + 32]), A.sigma[r + lane + 32]));
+        }
+      }
+    }
+    if (h0) A.delta[v * kBcB + lane] = d0;
+    if (h1) A.delta[v * kBcB + lane + 32] = d1;
+  }
+}
+
+// The batch's partial (sources in order, each source's own node excluded),
+// added to out in batch order.
+__global__ void bc_fold_k(const double* __restrict__ delta, const uint32_t* __restrict__ src,
+                          uint32_t nq, uint64_t n, double* __restrict__ out) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    double p = 0.0;
+    for (uint32_t q = 0; q < nq; q++)
+      if (src[q] != v) p = __dadd_rn(p, delta[v * kBcB + q]);
+    out[v] = __dadd_rn(out[v], p);
+  }
+}
+
+__global__ void inv_perm_k(const uint32_t* __restrict__ eid, uint64_t m, uint32_t* __restrict__ inv) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
+       k += (uint64_t)gridDim.x * blockDim.x)
+    inv[eid[k]] = (uint32_t)k;
+}
+
+__global__ void compose_k(const uint32_t* __restrict__ a, const uint32_t* __restrict__ inv, uint64_t m,
+                          uint32_t* __restrict__ out) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
+       k += (uint64_t)gridDim.x * blockDim.x)
+    out[k] = inv[a[k]];
+}
+
 }  // namespace
+
+// Unweighted betweenness over `sources`, 64 at a time, added into d_out.
+static void betweenness_batched(TopoImpl* t, const std::vector<uint32_t>& sources, double* d_out,
+                                cudaStream_t s) {
+  const uint64_t n = t->n, m = t->m;
+  ensure_in(t, s);
+  Scratch<uint32_t> in_to_out(m ? m : 1, s);
+  if (m) {
+    Scratch<uint32_t> inv(m, s);
+    inv_perm_k<<<grid_for(m), kBlock, 0, s>>>(t->out.eid.get(), m, inv.get());
+    UG_LAUNCH_CHECK();
+    compose_k<<<grid_for(m), kBlock, 0, s>>>(t->in.eid.get(), inv.get(), m, in_to_out.get());
+    UG_LAUNCH_CHECK();
+  }
+  Scratch<uint64_t> vis(n, s), fa(n, s), fb(n, s), dag(m ? m : 1, s);
+  Scratch<int32_t> hop(n * kBcB, s);
+  Scratch<double> sigma(n * kBcB, s), delta(n * kBcB, s);
+  Scratch<uint32_t> d_src(kBcB, s);
+  Scratch<unsigned> found(1, s);
+  BcBatchArgs a;
+  a.in_off = t->in.off.get();
+  a.in_src = t->in.tgt.get();
+  a.in_to_out = in_to_out.get();
+  a.out_off = t->out.off.get();
+  a.out_tgt = t->out.tgt.get();
+  a.n = n;
+  a.vis = vis.get();
+  a.hop = hop.get();
+  a.sigma = sigma.get();
+  a.delta = delta.get();
+  a.dag = dag.get();
+  a.found = found.get();
+  const unsigned gw = grid_for(n * 32, kBlock, 148u * 8u);
+  for (size_t c0 = 0; c0 < sources.size(); c0 += kBcB) {
+    const uint32_t nq = (uint32_t)std::min<size_t>(kBcB, sources.size() - c0);
+    a.qmask = nq == 64 ? ~0ull : ((1ull << nq) - 1ull);
+    UG_CUDA(cudaMemcpyAsync(d_src.get(), sources.data() + c0, nq * 4, cudaMemcpyHostToDevice, s));
+    UG_CUDA(cudaMemsetAsync(vis.get(), 0, n * 8, s));
+    UG_CUDA(cudaMemsetAsync(fa.get(), 0, n * 8, s));
+    UG_CUDA(cudaMemsetAsync(hop.get(), 0xFF, n * kBcB * 4, s));
+    UG_CUDA(cudaMemsetAsync(sigma.get(), 0, n * kBcB * 8, s));
+    UG_CUDA(cudaMemsetAsync(delta.get(), 0, n * kBcB * 8, s));
+    if (m) UG_CUDA(cudaMemsetAsync(dag.get(), 0, m * 8, s));
+    bc_seed_k<<<1, kBcB, 0, s>>>(d_src.get(), nq, vis.get(), fa.get(), hop.get(), sigma.get());
+    UG_LAUNCH_CHECK();
+    int32_t L = 0;
+    uint64_t* cur = fa.get();
+    uint64_t* nxt = fb.get();
+    while (true) {
+      a.level = L + 1;
+      a.front = cur;
+      a.next = nxt;
+      UG_CUDA(cudaMemsetAsync(found.get(), 0, 4, s));
+      bc_forward_k<<<gw, kBlock, 0, s>>>(a);
+      UG_LAUNCH_CHECK();
+      unsigned f = 0;
+      UG_CUDA(cudaMemcpyAsync(&f, found.get(), 4, cudaMemcpyDeviceToHost, s));
+      UG_CUDA(cudaStreamSynchronize(s));
+      if (!f) break;
+      L++;
+      std::swap(cur, nxt);
+    }
+    // nodes of the deepest level L have no successors (delta 0)
+    for (int32_t lvl = L - 1; lvl >= 0; lvl--) {
+      a.level = lvl;
+      bc_backward_k<<<gw, kBlock, 0, s>>>(a);
+      UG_LAUNCH_CHECK();
+    }
+    bc_fold_k<<<grid_for(n), kBlock, 0, s>>>(delta.get(), d_src.get(), nq, n, d_out);
+    UG_LAUNCH_CHECK();
+  }
+}
 
 struct BcState {
   Scratch<int32_t> hop;                 // unweighted BFS level (-1 = unreached)
@@ -345,6 +586,9 @@ void betweenness_run(TopoImpl* t, const double* d_weights, bool has_sample, doub
   } else {
     st.hop.alloc(n, s);
   }
+  if (!d_weights) {
+    betweenness_batched(t, sources, d_out, s);
+  } else {
   Scratch<double> acc(n, s);
   for (size_t c0 = 0; c0 < sources.size(); c0 += kSrcChunk) {
     UG_CUDA(cudaMemsetAsync(acc.get(), 0, n * 8, s));
@@ -353,6 +597,7 @@ void betweenness_run(TopoImpl* t, const double* d_weights, bool has_sample, doub
       brandes_source(t, d_weights ? w_out.get() : nullptr, sources[i], st, acc.get(), s);
     add_into_k<<<grid_for(n), kBlock, 0, s>>>(d_out, acc.get(), n);
     UG_LAUNCH_CHECK();
+  }
   }
   if (has_sample) {
     scale_k<<<grid_for(n), kBlock, 0, s>>>(d_out, n, (double)n / (double)sources.size());
