@@ -82,8 +82,9 @@ DAMPING, TOL, MAX_ITER = 0.85, 1e-6, 100
 WORKLOAD = "rmat22_pagerank"
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one pr_persistent_k launch on
-# this workload (prologue + 5 fixed iterations), from the ncu capture
-# summarised in profiles/pagerank_rmat22.md.
+# this workload (prologue + 5 fixed iterations), measured by
+#   ncu --set full --clock-control none -k regex:pr_persistent -s 3 -c 1 \
+#     python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --max-iter 5 --tol 0
 NCU_TRAFFIC = {"bytes_per_launch": 1_341_229_000 + 55_156_736, "iterations": 5}
 
 
@@ -184,8 +185,23 @@ def make_workload():
     return n, src, dst
 
 
+def rmat22_config(n, m, tol, max_iter, iters, world):
+    """The workload's config dict, identical in both arms."""
+    return {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": tol,
+            "max_iter": max_iter, "iterations": iters, "l2": "inputs larger than L2 (in-CSR 261 MB)",
+            "parallelism": "replicas" if world > 1 else "single"}
+
+
+REF_E2E_STEPS = 3
+
+
 def run_reference(args, rank, world):
-    """The reference algorithm on the host (CPU restatement of ursa-core)."""
+    """The reference algorithm on the host (CPU restatement of ursa-core).
+
+    value: pagerank to tol with the CSR and its transpose already built (the
+    warm kernel, as the device arm's value has its topology resident), one
+    call per step.  e2e: Topology::build + transpose + pagerank per step, on
+    REF_E2E_STEPS samples (the device arm's e2e also builds every step)."""
     if rank != 0:
         return
     from oracle import oracle as O
@@ -195,24 +211,35 @@ def run_reference(args, rank, world):
     O.set_threads(threads)
     n, src, dst = make_workload()
     m = int(src.size)
+    topo = O.Topology(n, src, dst)
+    topo.csr("in")  # the transpose, built once
 
-    def step():
+    def warm_step():
         t0 = time.perf_counter()
-        topo = O.Topology(n, src, dst)
-        _, it = O.pagerank(topo, DAMPING, MAX_ITER, TOL, return_iters=True)
+        _, it = O.pagerank(topo, DAMPING, args.max_iter, args.tol, return_iters=True)
+        return time.perf_counter() - t0, it
+
+    def e2e_step():
+        t0 = time.perf_counter()
+        t = O.Topology(n, src, dst)
+        t.csr("in")
+        _, it = O.pagerank(t, DAMPING, args.max_iter, args.tol, return_iters=True)
         dt = time.perf_counter() - t0
-        del topo
+        del t
         return dt, it
 
     for _ in range(args.warmup):
-        step()
+        warm_step()
     times, iters = [], []
     for _ in range(args.steps):
-        dt, it = step()
+        dt, it = warm_step()
         times.append(dt)
         iters.append(it)
+    del topo
+    e2e = [e2e_step() for _ in range(REF_E2E_STEPS)]
     total = sum(times)
     value = m * sum(iters) / total / 1e9
+    e2e_value = m * sum(it for _, it in e2e) / sum(dt for dt, _ in e2e) / 1e9
     line = {
         "impl": "reference",
         "metric": "pagerank_gteps",
@@ -227,20 +254,22 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": TOL,
-                   "max_iter": MAX_ITER, "iterations": iters[-1], "l2": "inputs larger than L2",
-                   "parallelism": "replicas" if world > 1 else "single"},
+        "config": rmat22_config(n, m, args.tol, args.max_iter, iters[-1] if iters else 0, world),
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": "port",
-                         "sample": "full Topology::build + transpose + pagerank to tol per step "
-                                   "(C restatement of ursa-core; the Rust crate cannot be built here)"},
-        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                         "sample": "pagerank to tol per step with the CSR and transpose prebuilt (C restatement "
+                                   "of ursa-core; the Rust crate cannot be built here)"},
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "ms_per_step": 1e3 * sum(dt for dt, _ in e2e) / len(e2e),
+                "sample": f"{REF_E2E_STEPS} steps of Topology::build + transpose + pagerank to tol"},
     }
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(n, src, dst):
-    """Warm CPU PageRank GTEPS of the oracle on this workload (bounded sample:
-    5 fixed power iterations with the CSR and transpose prebuilt)."""
+def oracle_check(n, src, dst, got, gpu_iters, max_iter, tol, want_baseline):
+    """PageRank of the oracle on the same graph and parameters: the device
+    ranks' error against it (L1 and max relative error vs the f64 oracle,
+    both iteration counts) and, when asked, the oracle's warm speed as the
+    CPU baseline (that same call, timed, CSR and transpose prebuilt)."""
     from oracle import oracle as O
 
     O.build()
@@ -248,12 +277,68 @@ def cpu_baseline(n, src, dst):
     O.set_threads(threads)
     topo = O.Topology(n, src, dst)
     topo.csr("in")  # prebuild the transpose (warm kernel)
-    iters = 5
     t0 = time.perf_counter()
-    O.pagerank(topo, DAMPING, iters, 0.0)
+    ref, it = O.pagerank(topo, DAMPING, max_iter, tol, return_iters=True)
     dt = time.perf_counter() - t0
-    return {"value": src.size * iters / dt / 1e9, "unit": "GTEPS", "cores": threads, "kind": "port",
-            "sample": f"{iters} warm power iterations (tol=0) on the same R-MAT-22 graph, CSR+transpose prebuilt"}
+    deltas = O.pagerank_deltas()
+    diff = np.abs(got - ref)
+    error = {"l1": float(diff.sum()),
+             "max_rel": float((diff / np.maximum(np.abs(ref), 1e-300)).max()) if ref.size else 0.0,
+             "iters": int(gpu_iters), "iters_oracle": int(it),
+             "oracle_last_delta": float(deltas[-1]) if deltas.size else None,
+             "reference": "oracle (C restatement of ursa-core pagerank.rs, f64) on the same graph"}
+    baseline = None
+    if want_baseline:
+        baseline = {"value": src.size * it / dt / 1e9, "unit": "GTEPS", "cores": threads, "kind": "port",
+                    "sample": f"one warm pagerank to tol ({it} iterations) on the same R-MAT-22 graph, "
+                              "CSR+transpose prebuilt"}
+    return error, baseline
+
+
+def e2e_phases(L, n, m, h_src, h_dst, h_out, params, reps=3):
+    """Where an end-to-end step's time goes (medians over reps, each phase
+    synchronised on its own): the H2D of the two endpoint columns from pinned
+    memory, the out-CSR + transpose build from device columns, the first
+    pagerank call on the new topology (its execution plan, the kernel, the
+    rank unpermute and the D2H of the ranks), the kernel alone (device
+    events), and the D2H of the n f64 ranks alone.  The e2e step itself
+    overlaps the destinations' H2D with the first radix passes."""
+    import torch
+
+    from ursa_b200 import PageRankStats, _lib
+
+    rec = {k: [] for k in ("h2d", "build", "pagerank_call", "kernel", "d2h")}
+    d_src = torch.empty(m, dtype=torch.int32, device="cuda")
+    d_dst = torch.empty(m, dtype=torch.int32, device="cuda")
+    d_out = torch.empty(n, dtype=torch.float64, device="cuda")
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d_src.copy_(h_src.view(torch.int32), non_blocking=True)
+        d_dst.copy_(h_dst.view(torch.int32), non_blocking=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        h = C.c_void_p()
+        _lib.check(L.ursa_gpu_topo_build_device(n, d_src.data_ptr(), d_dst.data_ptr(), m, None, C.byref(h)))
+        t2 = time.perf_counter()
+        st = PageRankStats()
+        try:
+            _lib.check(L.ursa_gpu_pagerank(h, C.byref(params), h_out.data_ptr(), C.byref(st)))
+        finally:
+            t3 = time.perf_counter()
+            L.ursa_gpu_topo_free(h)
+        torch.cuda.synchronize()
+        t4 = time.perf_counter()
+        h_out.copy_(d_out, non_blocking=True)
+        torch.cuda.synchronize()
+        t5 = time.perf_counter()
+        for k, v in (("h2d", t1 - t0), ("build", t2 - t1), ("pagerank_call", t3 - t2),
+                     ("kernel", st.device_ms * 1e-3), ("d2h", t5 - t4)):
+            rec[k].append(1e3 * v)
+    out = {k: statistics.median(v) for k, v in rec.items()}
+    out["h2d_gbs"] = 8 * m / (out["h2d"] * 1e-3) / 1e9
+    out["plan_and_unpermute"] = out["pagerank_call"] - out["kernel"] - out["d2h"]
+    return out
 
 
 BATCH_COUNT = 10_000
@@ -829,6 +914,18 @@ def run_suite(args, rank, world):
              cpu_edges / (c_ms * 1e-3) / 1e9, {"exact": bool(exact), "sources_checked": k_cpu},
              int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
              cpu_note="the oracle's BFS is one serial walk per source (as bfs.rs)")
+        # the same sources in one bit-parallel traversal (ursa_gpu_bfs_distances_multi)
+        multi = pinned(len(srcs) * n, torch.int32)
+        src_arr = np.asarray(srcs, np.uint32)
+        t = gpu(lambda: _lib.check(L.ursa_gpu_bfs_distances_multi(h, src_arr.ctypes.data, len(srcs), 0,
+                                                                  multi.ctypes.data)))
+        mrows = multi.reshape(len(srcs), n)
+        same = all(np.array_equal(mrows[i], dist[i]) for i in range(len(srcs)))
+        emit(cfg, f"bfs_multi_x{len(srcs)}", t, teps_edges / (t * 1e-3) / 1e9, "GTEPS", c_ms,
+             cpu_edges / (c_ms * 1e-3) / 1e9, cpu_edges / (c_ms * 1e-3) / 1e9,
+             {"equal_to_single_source": bool(same), "sources": len(srcs)},
+             int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
+             note="all sources in one traversal; the result rows cross the host link inside the timed span")
 
         # ---- weak components
         cc = pinned(n, torch.int32)
@@ -907,11 +1004,17 @@ SERVE_WORKLOAD = "serve_rmat24_uploads"
 SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
 
 
+SERVE_MIX = {"shortest_path": 0.45, "bfs": 0.05, "hop2": 0.30, "pagerank": 0.20}
+
+
 def serve_queries(n, rng, count):
     """(kind, a, b) with kind 0 = shortest_path(a, b), 1 = hop(a, k=2),
-    2 = pagerank on the upload picked by b (a uniform draw)."""
+    2 = pagerank on the upload picked by b (a uniform draw), 3 = bfs from a
+    (Out).  The bfs/shortest_path half of the stream is 5% bfs: a bfs answer
+    is n i32 distances (67 MB at R-MAT-24), so bfs throughput is bound by the
+    host link (~800/s) whatever the GPU does."""
     r = rng.random(count)
-    kind = np.where(r < 0.5, 0, np.where(r < 0.8, 1, 2))
+    kind = np.where(r < 0.45, 0, np.where(r < 0.5, 3, np.where(r < 0.8, 1, 2)))
     a = rng.integers(0, n, count)
     b = rng.integers(0, n, count)
     return kind, a, b
@@ -936,7 +1039,7 @@ def run_serve(args, rank, world):
     uoff = np.concatenate([[0], np.cumsum(uk)]).astype(np.int64)
     ups = [(int(un[i]), us[uoff[i]:uoff[i + 1]], ud[uoff[i]:uoff[i + 1]]) for i in range(len(un))]
     srv = Server(topo, path_lanes=4, path_slots=16, hop_lanes=4, hop_slots=16, pr_lanes=2, pr_slots=32,
-                 pr_max_nodes=65536, hbm_reserve_bytes=16 << 30)
+                 pr_max_nodes=65536, hbm_reserve_bytes=16 << 30, bfs_lanes=1, bfs_slots=16)
     live, live_lock = [], threading.Lock()
     stop_up = threading.Event()
 
@@ -995,6 +1098,8 @@ def run_serve(args, rank, world):
                 tickets.append(srv.shortest_path(int(a[i]), int(b[i])))
             elif kind[i] == 1:
                 tickets.append(srv.hop(int(a[i]), 2))
+            elif kind[i] == 3:
+                tickets.append(srv.bfs(int(a[i]), 0))
             else:
                 # pick and submit under the lock: the uploader removes an id
                 # from `live` (under it) before releasing the graph, and the
@@ -1014,11 +1119,32 @@ def run_serve(args, rank, world):
         out = {"completed_qps": len(infos) / ((t_last - t_first) * 1e-6),
                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                "errors": int(sum(1 for x in infos if x.status != 0))}
-        for k, name in ((0, "shortest_path"), (1, "hop2"), (2, "pagerank")):
+        for k, name in ((0, "shortest_path"), (1, "hop2"), (2, "pagerank"), (3, "bfs")):
             sel = lat[kind == k]
             if sel.size:
                 out[name] = {"p50_ms": float(np.percentile(sel, 50)), "p99_ms": float(np.percentile(sel, 99))}
         return out
+
+    def single_type(k, count, seed):
+        """Closed loop of one query type on the server: its capacity."""
+        rng = np.random.default_rng(seed)
+        kind = np.full(count, k)
+        a = rng.integers(0, n, count)
+        b = rng.integers(0, n, count)
+        tickets = []
+        for i in range(count):
+            if k == 0:
+                tickets.append(srv.shortest_path(int(a[i]), int(b[i])))
+            elif k == 1:
+                tickets.append(srv.hop(int(a[i]), 2))
+            elif k == 3:
+                tickets.append(srv.bfs(int(a[i]), 0))
+            else:
+                with live_lock:
+                    gid = live[int(b[i]) % len(live)]
+                    tickets.append(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
+        infos = [srv.result(t, timeout_s=600) for t in tickets]
+        return summarize(infos, kind)
 
     try:
         drive(2000, 2000, 1)  # warm-up
@@ -1045,6 +1171,8 @@ def run_serve(args, rank, world):
         infos, offered, kind = drive(1e9, 60000, 999)
         total_q += 60000
         closed = summarize(infos, kind)
+        per_type_server = {name: single_type(k, cnt, 700 + k) for k, name, cnt in
+                           ((0, "shortest_path", 20000), (1, "hop2", 20000), (2, "pagerank", 5000), (3, "bfs", 400))}
         clocks = sampler.stop() if sampler else None
         launches = L.ursa_gpu_launch_count() - launches0
         stats = srv.stats()
@@ -1059,7 +1187,10 @@ def run_serve(args, rank, world):
     upt.join(timeout=30)
     srv.close()
 
-    # the plain path: one query per C-ABI call, 4 host threads, closed loop
+    # the plain path: one query per C-ABI call, 4 host threads, closed loop;
+    # per type, and for shortest_path both the reference's algorithm
+    # (unidirectional exact-order BFS) and the server's (bidirectional, one
+    # launch per query)
     plain_topos = {}
     rng = np.random.default_rng(4242)
     kind, a, b = serve_queries(n, rng, 2000)
@@ -1071,14 +1202,25 @@ def run_serve(args, rank, world):
     keys = list(plain_topos)
     lat = np.zeros(len(kind))
 
+    tls = threading.local()
+
+    def plain_call(k, x, y):
+        if k == 0:
+            algo.shortest_path(topo, x, y)
+        elif k == 1:
+            algo.k_hop(topo, [x], 2)
+        elif k == 3:
+            if not hasattr(tls, "buf"):
+                tls.buf = np.empty(n, np.int32)
+            _lib.check(L.ursa_gpu_bfs_distances(topo.handle, x, 0, tls.buf.ctypes.data))
+        elif k == 4:
+            algo.shortest_path_bidirectional(topo, x, y)
+        else:
+            algo.pagerank(plain_topos[keys[y % len(keys)]], pr_params)
+
     def plain_one(i):
         t0 = time.perf_counter()
-        if kind[i] == 0:
-            algo.shortest_path(topo, int(a[i]), int(b[i]))
-        elif kind[i] == 1:
-            algo.k_hop(topo, [int(a[i])], 2)
-        else:
-            algo.pagerank(plain_topos[keys[int(b[i]) % len(keys)]], pr_params)
+        plain_call(int(kind[i]), int(a[i]), int(b[i]))
         lat[i] = time.perf_counter() - t0
 
     import concurrent.futures as cf
@@ -1091,6 +1233,36 @@ def run_serve(args, rank, world):
     plain = {"completed_qps": len(kind) / plain_s, "p50_ms": float(np.percentile(lat, 50) * 1e3),
              "p99_ms": float(np.percentile(lat, 99) * 1e3), "queries": int(len(kind)), "threads": 4,
              "note": "closed loop; latency is the per-call service time (no queueing)"}
+
+    def plain_type(k, count, seed):
+        r = np.random.default_rng(seed)
+        xs, ys = r.integers(0, n, count), r.integers(0, n, count)
+        lt = np.zeros(count)
+
+        def one(i):
+            t1 = time.perf_counter()
+            plain_call(k, int(xs[i]), int(ys[i]))
+            lt[i] = time.perf_counter() - t1
+
+        with cf.ThreadPoolExecutor(4) as ex:
+            list(ex.map(one, range(min(count, 20))))
+            t1 = time.perf_counter()
+            list(ex.map(one, range(count)))
+            dt = time.perf_counter() - t1
+        return {"completed_qps": count / dt, "p50_ms": float(np.percentile(lt, 50) * 1e3),
+                "p99_ms": float(np.percentile(lt, 99) * 1e3), "queries": count}
+
+    plain_types = {"shortest_path": plain_type(0, 400, 801), "shortest_path_same_algorithm": plain_type(4, 2000, 802),
+                   "hop2": plain_type(1, 2000, 803), "pagerank": plain_type(2, 400, 804), "bfs": plain_type(3, 100, 805)}
+    per_type = {}
+    for name, srv_row in per_type_server.items():
+        row = {"server": srv_row, "plain": plain_types[name],
+               "speedup": srv_row["completed_qps"] / plain_types[name]["completed_qps"]}
+        if name == "shortest_path":
+            row["plain_same_algorithm"] = plain_types["shortest_path_same_algorithm"]
+            row["speedup_same_algorithm"] = (srv_row["completed_qps"] /
+                                             plain_types["shortest_path_same_algorithm"]["completed_qps"])
+        per_type[name] = row
 
     if rank == 0:
         best = max(sweep, key=lambda r: r["completed_qps"])
@@ -1109,13 +1281,14 @@ def run_serve(args, rank, world):
             "data": "synthetic",
             "config": {"workload": SERVE_WORKLOAD, "resident_nodes": n, "resident_edges": m,
                        "uploads": "Poisson 200/s, 2 s lifetime, rmat_batch sizes",
-                       "mix": {"shortest_path": 0.5, "hop2": 0.3, "pagerank": 0.2},
-                       "lanes": {"shortest_path": [4, 16], "hop": [4, 16], "pagerank": [2, 32]}},
+                       "mix": SERVE_MIX,
+                       "lanes": {"shortest_path": [4, 16], "hop": [4, 16], "pagerank": [2, 32], "bfs": [1, 16]}},
             "closed_loop": closed,
             "sweep": sweep,
             "best_open_loop": {"rate_qps": best["rate_qps"], "completed_qps": best["completed_qps"]},
             "plain_one_query_per_launch": plain,
             "speedup_vs_plain": closed["completed_qps"] / plain["completed_qps"],
+            "per_type": per_type,
             "e2e": {"value": closed["completed_qps"], "unit": "queries/s", "h2d_bytes_per_step": None,
                     "d2h_bytes_per_step": None,
                     "note": "every query is submitted from and returned to host memory through the C ABI"},
@@ -1429,6 +1602,8 @@ def main():
             it = e2e_step()
             e2e_times.append(time.perf_counter() - t0)
             e2e_iters.append(it)
+    phases = e2e_phases(L, n, m, h_src, h_dst, h_out, params) if e2e_times else None
+    got = d_out.cpu().numpy()
 
     # ---- max over ranks
     t_dev, t_e2e, edges_iters_all, e2e_edges_all = combine_replicas(
@@ -1459,12 +1634,13 @@ def main():
             "vs_baseline": None,
             "dtype": "f32-compensated SpMV, f64 ranks/residual",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_nodes": n, "n_edges": m, "damping": DAMPING, "tol": args.tol,
-                       "max_iter": args.max_iter, "iterations": iters, "l2": "inputs larger than L2 (in-CSR 261 MB)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+            "config": rmat22_config(n, m, args.tol, args.max_iter, iters, world),
             "e2e": None if not e2e_times else {"value": e2e_edges_all / t_e2e / 1e9, "unit": "GTEPS",
                     "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 8 * n,
-                    "ms_per_step": 1e3 * t_e2e / args.steps},
+                    "ms_per_step": 1e3 * t_e2e / args.steps,
+                    "step_ms_min_median_max": [1e3 * min(e2e_times), 1e3 * statistics.median(e2e_times),
+                                               1e3 * max(e2e_times)],
+                    "phases_ms": phases},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
@@ -1472,8 +1648,11 @@ def main():
                          "algorithmic_bytes_per_launch": alg},
             "clocks": clocks,
         }
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(n, src, dst)
+        error, baseline = oracle_check(n, src, dst, got, iters, args.max_iter, args.tol,
+                                       world == 1 and not args.no_cpu_baseline)
+        line["error"] = error
+        if baseline:
+            line["cpu_baseline"] = baseline
         print(json.dumps(line), flush=True)
     del topo
     if dist:
