@@ -770,6 +770,10 @@ def run_suite(args, rank, world):
     peak, peak_kind = load_peaks()
     reps = max(args.steps, 1)
     only = set(args.suite.split(",")) if args.suite else set(SUITE)
+    kern = set(args.suite_kernels.split(",")) if args.suite_kernels else None
+
+    def want(name):  # --suite-kernels: run only these sections (profiling runs)
+        return kern is None or name in kern
 
     def pinned(n, dtype):
         return torch.empty(max(n, 1), dtype=dtype).pin_memory().numpy()[:n]
@@ -829,115 +833,122 @@ def run_suite(args, rank, world):
         n, s, d, w = graph(cfg)
         m = int(s.size)
         # ---- CSR build and transpose (device arrays in; Topology::build + incoming)
-        d_s = torch.from_numpy(s).cuda()
-        d_d = torch.from_numpy(d).cuda()
-        tb = []
-        for r in range(reps + 1):  # each build freed before the next (outside the timed span)
-            h = C.c_void_p()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(lib_stream)
-            _lib.check(L.ursa_gpu_topo_build_device(n, d_s.data_ptr(), d_d.data_ptr(), m, C.c_void_p(sp.value),
-                                                    C.byref(h)))
-            e1.record(lib_stream)
-            e1.synchronize()
-            if r:
-                tb.append(e0.elapsed_time(e1))
-            L.ursa_gpu_topo_free(h)
-        t_build = statistics.median(tb)
-        del d_s, d_d
+        if want("build"):
+            d_s = torch.from_numpy(s).cuda()
+            d_d = torch.from_numpy(d).cuda()
+            tb = []
+            for r in range(reps + 1):  # each build freed before the next (outside the timed span)
+                h = C.c_void_p()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(lib_stream)
+                _lib.check(L.ursa_gpu_topo_build_device(n, d_s.data_ptr(), d_d.data_ptr(), m, C.c_void_p(sp.value),
+                                                        C.byref(h)))
+                e1.record(lib_stream)
+                e1.synchronize()
+                if r:
+                    tb.append(e0.elapsed_time(e1))
+                L.ursa_gpu_topo_free(h)
+            t_build = statistics.median(tb)
+            del d_s, d_d
         g = Topology.build(n, s, d)
         cb_ms, ot = cpu(lambda: O.Topology(n, s, d), cores)
         ct_ms, _ = cpu(lambda: ot.csr("in"), cores)
-        go, oo = g.out(), ot.csr("out")
-        gi, oi = g.incoming(), ot.csr("in")
-        same = all(np.array_equal(a, b) for a, b in [(go.offsets, oo[0]), (go.targets, oo[1]), (go.edge_ids, oo[2]),
-                                                     (gi.offsets, oi[0]), (gi.targets, oi[1]), (gi.edge_ids, oi[2])])
-        emit(cfg, "csr_build_and_transpose", t_build, m / (t_build * 1e-3), "edges/s", cb_ms + ct_ms,
-             m / ((cb_ms + ct_ms) * 1e-3), None, {"byte_identical": bool(same)}, 2 * (20 * m + 8 * (n + 1)),
-             input="device src/dst arrays",
-             note="the device build sorts the rows by source and by destination in one call (the endpoint "
-                  "columns are already in row order on the device); the oracle builds, then transposes",
-             cpu_build_ms=cb_ms, cpu_transpose_ms=ct_ms)
+        if want("build"):
+            go, oo = g.out(), ot.csr("out")
+            gi, oi = g.incoming(), ot.csr("in")
+            same = all(np.array_equal(a, b) for a, b in [(go.offsets, oo[0]), (go.targets, oo[1]),
+                                                         (go.edge_ids, oo[2]), (gi.offsets, oi[0]),
+                                                         (gi.targets, oi[1]), (gi.edge_ids, oi[2])])
+            emit(cfg, "csr_build_and_transpose", t_build, m / (t_build * 1e-3), "edges/s", cb_ms + ct_ms,
+                 m / ((cb_ms + ct_ms) * 1e-3), None, {"byte_identical": bool(same)}, 2 * (20 * m + 8 * (n + 1)),
+                 input="device src/dst arrays",
+                 note="the device build sorts the rows by source and by destination in one call (the endpoint "
+                      "columns are already in row order on the device); the oracle builds, then transposes",
+                 cpu_build_ms=cb_ms, cpu_transpose_ms=ct_ms)
         h = g.handle
         deg_out = pinned(n, torch.int32)
 
         # ---- degree
-        for dname, dval in (("out", 0), ("in", 1)):
-            t = gpu(lambda: _lib.check(L.ursa_gpu_degree(h, dval, deg_out.ctypes.data)))
-            c_ms, ref = cpu(lambda: O.degree(ot, dname), cores)
-            emit(cfg, f"degree_{dname}", t, n / (t * 1e-3), "nodes/s", c_ms, n / (c_ms * 1e-3), None,
-                 {"exact": bool(np.array_equal(deg_out.view(np.uint32), ref))}, 4 * (n + 1) + 4 * n)
+        if want("degree"):
+            for dname, dval in (("out", 0), ("in", 1)):
+                t = gpu(lambda: _lib.check(L.ursa_gpu_degree(h, dval, deg_out.ctypes.data)))
+                c_ms, ref = cpu(lambda: O.degree(ot, dname), cores)
+                emit(cfg, f"degree_{dname}", t, n / (t * 1e-3), "nodes/s", c_ms, n / (c_ms * 1e-3), None,
+                     {"exact": bool(np.array_equal(deg_out.view(np.uint32), ref))}, 4 * (n + 1) + 4 * n)
         outdeg = O.degree(ot, "out")
 
         # ---- pagerank (plain; weighted on C3)
-        for weighted in ((False, True) if w is not None else (False,)):
-            pr = pinned(n, torch.float64)
-            stt = PageRankStats()
-            par = PageRankParams(DAMPING, MAX_ITER, TOL)
-            if weighted:
-                fn = lambda: _lib.check(L.ursa_gpu_pagerank_weighted(h, w.ctypes.data, m, C.byref(par),
-                                                                     pr.ctypes.data, C.byref(stt)))
-            else:
-                fn = lambda: _lib.check(L.ursa_gpu_pagerank(h, C.byref(par), pr.ctypes.data, C.byref(stt)))
-            t = gpu(fn)
-            iters = stt.iterations
-            if weighted:
-                c_ms, (ref, oit) = cpu(lambda: O.pagerank_weighted(ot, w, DAMPING, MAX_ITER, TOL, True), cores)
-                c1_ms, _ = cpu(lambda: O.pagerank_weighted(ot, w, DAMPING, 1, 0.0), 1)
-            else:
-                c_ms, (ref, oit) = cpu(lambda: O.pagerank(ot, DAMPING, MAX_ITER, TOL, True), cores)
-                c1_ms, _ = cpu(lambda: O.pagerank(ot, DAMPING, 1, 0.0), 1)
-            err = rel_err(pr, ref)
-            err.update({"iterations": iters, "oracle_iterations": int(oit)})
-            alg = algorithmic_bytes(n, m, iters) + (4 * m * iters if weighted else 0)
-            emit(cfg, "pagerank_weighted" if weighted else "pagerank", t, m * iters / (t * 1e-3) / 1e9, "GTEPS",
-                 c_ms, m * oit / (c_ms * 1e-3) / 1e9, m / (c1_ms * 1e-3) / 1e9, err, alg)
+        if want("pagerank"):
+            for weighted in ((False, True) if w is not None else (False,)):
+                pr = pinned(n, torch.float64)
+                stt = PageRankStats()
+                par = PageRankParams(DAMPING, MAX_ITER, TOL)
+                if weighted:
+                    fn = lambda: _lib.check(L.ursa_gpu_pagerank_weighted(h, w.ctypes.data, m, C.byref(par),
+                                                                         pr.ctypes.data, C.byref(stt)))
+                else:
+                    fn = lambda: _lib.check(L.ursa_gpu_pagerank(h, C.byref(par), pr.ctypes.data, C.byref(stt)))
+                t = gpu(fn)
+                iters = stt.iterations
+                if weighted:
+                    c_ms, (ref, oit) = cpu(lambda: O.pagerank_weighted(ot, w, DAMPING, MAX_ITER, TOL, True), cores)
+                    c1_ms, _ = cpu(lambda: O.pagerank_weighted(ot, w, DAMPING, 1, 0.0), 1)
+                else:
+                    c_ms, (ref, oit) = cpu(lambda: O.pagerank(ot, DAMPING, MAX_ITER, TOL, True), cores)
+                    c1_ms, _ = cpu(lambda: O.pagerank(ot, DAMPING, 1, 0.0), 1)
+                err = rel_err(pr, ref)
+                err.update({"iterations": iters, "oracle_iterations": int(oit)})
+                alg = algorithmic_bytes(n, m, iters) + (4 * m * iters if weighted else 0)
+                emit(cfg, "pagerank_weighted" if weighted else "pagerank", t, m * iters / (t * 1e-3) / 1e9, "GTEPS",
+                     c_ms, m * oit / (c_ms * 1e-3) / 1e9, m / (c1_ms * 1e-3) / 1e9, err, alg)
 
         # ---- BFS from sampled sources with out-degree > 0
         have_out = np.flatnonzero(outdeg > 0)
         k_src = {"C1": 8, "C2": 64, "C3": 8}[cfg]
         srcs = [int(have_out[i]) for i in O.sample_indices(have_out.size, k_src, {"C1": 1, "C2": 2, "C3": 3}[cfg])]
-        dist = [pinned(n, torch.int32) for _ in srcs]
+        if want("bfs"):
+            dist = [pinned(n, torch.int32) for _ in srcs]
 
-        def bfs_all():
-            for x, buf in zip(srcs, dist):
-                _lib.check(L.ursa_gpu_bfs_distances(h, x, 0, buf.ctypes.data))
+            def bfs_all():
+                for x, buf in zip(srcs, dist):
+                    _lib.check(L.ursa_gpu_bfs_distances(h, x, 0, buf.ctypes.data))
 
-        t = gpu(bfs_all)
-        teps_edges = sum(int(outdeg[np.asarray(dd) >= 0].sum()) for dd in dist)
-        k_cpu = min(len(srcs), 8)
-        c_ms, refs = cpu(lambda: [O.bfs_distances(ot, x, "out") for x in srcs[:k_cpu]], cores)
-        exact = all(np.array_equal(dist[i], refs[i]) for i in range(k_cpu))
-        cpu_edges = sum(int(outdeg[r >= 0].sum()) for r in refs)
-        touched = teps_edges / max(len(srcs), 1)
-        emit(cfg, f"bfs_x{len(srcs)}", t, teps_edges / (t * 1e-3) / 1e9, "GTEPS", c_ms, cpu_edges / (c_ms * 1e-3) / 1e9,
-             cpu_edges / (c_ms * 1e-3) / 1e9, {"exact": bool(exact), "sources_checked": k_cpu},
-             int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
-             cpu_note="the oracle's BFS is one serial walk per source (as bfs.rs)")
-        # the same sources in one bit-parallel traversal (ursa_gpu_bfs_distances_multi)
-        multi = pinned(len(srcs) * n, torch.int32)
-        src_arr = np.asarray(srcs, np.uint32)
-        t = gpu(lambda: _lib.check(L.ursa_gpu_bfs_distances_multi(h, src_arr.ctypes.data, len(srcs), 0,
-                                                                  multi.ctypes.data)))
-        mrows = multi.reshape(len(srcs), n)
-        same = all(np.array_equal(mrows[i], dist[i]) for i in range(len(srcs)))
-        emit(cfg, f"bfs_multi_x{len(srcs)}", t, teps_edges / (t * 1e-3) / 1e9, "GTEPS", c_ms,
-             cpu_edges / (c_ms * 1e-3) / 1e9, cpu_edges / (c_ms * 1e-3) / 1e9,
-             {"equal_to_single_source": bool(same), "sources": len(srcs)},
-             int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
-             note="all sources in one traversal; the result rows cross the host link inside the timed span")
+            t = gpu(bfs_all)
+            teps_edges = sum(int(outdeg[np.asarray(dd) >= 0].sum()) for dd in dist)
+            k_cpu = min(len(srcs), 8)
+            c_ms, refs = cpu(lambda: [O.bfs_distances(ot, x, "out") for x in srcs[:k_cpu]], cores)
+            exact = all(np.array_equal(dist[i], refs[i]) for i in range(k_cpu))
+            cpu_edges = sum(int(outdeg[r >= 0].sum()) for r in refs)
+            touched = teps_edges / max(len(srcs), 1)
+            emit(cfg, f"bfs_x{len(srcs)}", t, teps_edges / (t * 1e-3) / 1e9, "GTEPS", c_ms, cpu_edges / (c_ms * 1e-3) / 1e9,
+                 cpu_edges / (c_ms * 1e-3) / 1e9, {"exact": bool(exact), "sources_checked": k_cpu},
+                 int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
+                 cpu_note="the oracle's BFS is one serial walk per source (as bfs.rs)")
+            # the same sources in one bit-parallel traversal (ursa_gpu_bfs_distances_multi)
+            multi = pinned(len(srcs) * n, torch.int32)
+            src_arr = np.asarray(srcs, np.uint32)
+            t = gpu(lambda: _lib.check(L.ursa_gpu_bfs_distances_multi(h, src_arr.ctypes.data, len(srcs), 0,
+                                                                      multi.ctypes.data)))
+            mrows = multi.reshape(len(srcs), n)
+            same = all(np.array_equal(mrows[i], dist[i]) for i in range(len(srcs)))
+            emit(cfg, f"bfs_multi_x{len(srcs)}", t, teps_edges / (t * 1e-3) / 1e9, "GTEPS", c_ms,
+                 cpu_edges / (c_ms * 1e-3) / 1e9, cpu_edges / (c_ms * 1e-3) / 1e9,
+                 {"equal_to_single_source": bool(same), "sources": len(srcs)},
+                 int(len(srcs) * (4 * (n + 1) + 4 * touched + 4 * n)), sources=len(srcs),
+                 note="all sources in one traversal; the result rows cross the host link inside the timed span")
 
         # ---- weak components
-        cc = pinned(n, torch.int32)
-        t = gpu(lambda: _lib.check(L.ursa_gpu_connected_components_weak(h, cc.ctypes.data)))
-        c_ms, ref = cpu(lambda: O.connected_components_weak(ot), cores)
-        exact = bool(np.array_equal(canon(cc.view(np.uint32)), canon(ref)))
-        emit(cfg, "connected_components_weak", t, m / (t * 1e-3), "edges/s", c_ms, m / (c_ms * 1e-3),
-             m / (c_ms * 1e-3), {"same_partition": exact}, 4 * m + 4 * (n + 1) + 16 * n,
-             cpu_note="union-find is serial in the reference")
+        if want("cc"):
+            cc = pinned(n, torch.int32)
+            t = gpu(lambda: _lib.check(L.ursa_gpu_connected_components_weak(h, cc.ctypes.data)))
+            c_ms, ref = cpu(lambda: O.connected_components_weak(ot), cores)
+            exact = bool(np.array_equal(canon(cc.view(np.uint32)), canon(ref)))
+            emit(cfg, "connected_components_weak", t, m / (t * 1e-3), "edges/s", c_ms, m / (c_ms * 1e-3),
+                 m / (c_ms * 1e-3), {"same_partition": exact}, 4 * m + 4 * (n + 1) + 16 * n,
+                 cpu_note="union-find is serial in the reference")
 
         # ---- triangles and clustering (C1, C2)
-        if cfg in ("C1", "C2"):
+        if cfg in ("C1", "C2") and want("tc"):
             ms_len = C.c_uint64()
             _lib.check(L.ursa_gpu_topo_undirected_len(h, C.byref(ms_len)))
             m_s = int(ms_len.value)
@@ -963,7 +974,7 @@ def run_suite(args, rank, world):
                  (m_s / (cc_ms * 1e-3)) if cc_ms else None, None, e_c, 4 * m_s + 8 * (n + 1) + 16 * n)
 
         # ---- weighted shortest paths and betweenness (C3)
-        if cfg == "C3":
+        if cfg == "C3" and want("sssp"):
             dd = pinned(n, torch.float64)
             s0 = srcs[0]
             t = gpu(lambda: _lib.check(L.ursa_gpu_dijkstra_distances(h, w.ctypes.data, m, s0, 0, dd.ctypes.data)))
@@ -983,6 +994,7 @@ def run_suite(args, rank, world):
             ok = oref is not None and k == len(oref[0]) and bool(np.array_equal(costs[:k], np.asarray(oref[1])))
             emit(cfg, "shortest_path_weighted_with_cost", t, None, None, c_ms, None, None,
                  {"cost_exact": ok, "path_len": k})
+        if cfg == "C3" and want("bc"):
             frac = 2.0 ** -12  # 256 sources at n = 2^20
             for weighted in (False, True):
                 bc = pinned(n, torch.float64)
@@ -1479,6 +1491,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="batch workload: keep the default launch shapes")
     ap.add_argument("--no-plain", action="store_true", help="batch workload: skip the per-graph plain loop")
     ap.add_argument("--suite", default="", help="suite workload: comma-separated configs (C1,C2,C3)")
+    ap.add_argument("--suite-kernels", default="",
+                    help="suite workload: only these sections (build,degree,pagerank,bfs,cc,tc,sssp,bc)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
