@@ -38,6 +38,7 @@ namespace {
 
 constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;
 constexpr uint32_t kSrcChunk = 64;  // betweenness.rs:51
+constexpr bool kBatchedWeighted = true;  // weighted sources 64 at a time (else one by one)
 
 // ---------------------------------------------------------------- rng.rs
 constexpr uint64_t kDefaultSeed = 0x5EED5EED5EED5EEDull;  // rng.rs:9
@@ -375,6 +376,192 @@ __global__ void bc_fold_k(const double* __restrict__ delta, const uint32_t* __re
   }
 }
 
+// ---- weighted, 64 sources at once -----------------------------------------
+// brandes_from_weighted (:278-339) for the batch: distances by a multi-source
+// frontier Bellman-Ford (lanes are sources; atomicMin on the bit patterns of
+// non-negative f64, whose fixpoint is Dijkstra's distances); then the tight
+// DAG per source (fl(dist[u] + w) == dist[v] exactly, the reference's tie
+// rule; zero-weight ties ordered by id) as a mask per out-CSR slot; then
+// sigma in rounds over that DAG -- a (node, source) is settled once every
+// tight predecessor was settled in an earlier round, and sigma is the sum
+// over them -- with the round as the node's level for the backward pass.
+struct BcwArgs {
+  const uint32_t* out_off;
+  const uint32_t* out_tgt;
+  const double* w_out;        // per out-CSR slot
+  const uint32_t* in_off;
+  const uint32_t* in_src;
+  const uint32_t* in_to_out;
+  uint64_t n;
+  uint64_t qmask;
+  unsigned long long* dist;   // n x 64 bit patterns
+  const uint64_t* flag_cur;   // sources whose distance at v fell last round
+  uint64_t* flag_next;
+  uint64_t* dag;              // per out-CSR slot: sources for which the edge is tight
+  uint64_t* reach;            // per node: sources that reach it
+  const uint64_t* done_prev;
+  uint64_t* done_next;
+  double* sigma;
+  int32_t* round;             // n x 64: the round a (node, source) settled, -1 = never
+  int32_t r;
+  unsigned* found;
+};
+
+__global__ void bcw_seed_k(const uint32_t* __restrict__ src, uint32_t nq, unsigned long long* dist,
+                           uint64_t* flag, uint64_t* done, int32_t* round, double* sigma) {
+  const uint32_t q = threadIdx.x;
+  if (q >= nq) return;
+  const uint32_t s = src[q];
+  dist[(uint64_t)s * kBcB + q] = 0ull;  // +0.0
+  atomicOr((unsigned long long*)(flag + s), 1ull << q);
+  atomicOr((unsigned long long*)(done + s), 1ull << q);
+  round[(uint64_t)s * kBcB + q] = 0;
+  sigma[(uint64_t)s * kBcB + q] = 1.0;
+}
+
+// One Bellman-Ford round: every (v, source) whose distance fell last round
+// relaxes v's out-edges.
+__global__ void bcw_relax_k(BcwArgs A) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  bool any = false;
+  for (uint64_t v = gw; v < A.n; v += nw) {
+    const uint64_t fl = A.flag_cur[v];
+    if (!fl) continue;
+    const bool f0 = (fl >> lane) & 1ull, f1 = (fl >> (lane + 32)) & 1ull;
+    const double d0 = f0 ? __longlong_as_double((long long)A.dist[v * kBcB + lane]) : 0.0;
+    const double d1 = f1 ? __longlong_as_double((long long)A.dist[v * kBcB + lane + 32]) : 0.0;
+    const uint32_t b = A.out_off[v], e = A.out_off[v + 1];
+    for (uint32_t k0 = b; k0 < e; k0 += 8) {
+      uint32_t wl = 0;
+      double xl = 0.0;
+      if (lane < 8 && k0 + lane < e) {
+        wl = A.out_tgt[k0 + lane];
+        xl = A.w_out[k0 + lane];
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if (k0 + j >= e) break;
+        const uint32_t w = __shfl_sync(0xffffffffu, wl, j);
+        const double x = __shfl_sync(0xffffffffu, xl, j);
+        bool low0 = false, low1 = false;
+        if (f0) {
+          const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(d0, x));
+          low0 = nd < atomicMin(&A.dist[(uint64_t)w * kBcB + lane], nd);
+        }
+        if (f1) {
+          const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(d1, x));
+          low1 = nd < atomicMin(&A.dist[(uint64_t)w * kBcB + lane + 32], nd);
+        }
+        const uint64_t lowered = (uint64_t)__ballot_sync(0xffffffffu, low0) |
+                                 ((uint64_t)__ballot_sync(0xffffffffu, low1) << 32);
+        if (lowered) {
+          any = true;
+          if (lane == 0) atomicOr((unsigned long long*)(A.flag_next + w), lowered);
+        }
+      }
+    }
+  }
+  if (lane == 0 && any) atomicOr(A.found, 1u);
+}
+
+__device__ __forceinline__ bool tight_bits(unsigned long long du, unsigned long long dv, double x,
+                                           uint32_t u, uint32_t v) {
+  if (du == kInfBits || u == v) return false;
+  const unsigned long long nd = (unsigned long long)__double_as_longlong(
+      __dadd_rn(__longlong_as_double((long long)du), x));
+  if (nd != dv) return false;
+  return du < dv || (du == dv && u < v);  // zero weights: keep the DAG acyclic
+}
+
+// Tight mask of every out-slot, and the sources that reach each node.
+__global__ void bcw_tight_k(BcwArgs A) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t u = gw; u < A.n; u += nw) {
+    const unsigned long long du0 = A.dist[u * kBcB + lane], du1 = A.dist[u * kBcB + lane + 32];
+    const uint64_t reach = ((uint64_t)__ballot_sync(0xffffffffu, du0 != kInfBits) |
+                            ((uint64_t)__ballot_sync(0xffffffffu, du1 != kInfBits) << 32)) & A.qmask;
+    if (lane == 0) A.reach[u] = reach;
+    if (!reach) continue;
+    const uint32_t b = A.out_off[u], e = A.out_off[u + 1];
+    for (uint32_t k = b; k < e; k++) {
+      const uint32_t v = A.out_tgt[k];
+      const double x = A.w_out[k];
+      const bool t0 = tight_bits(du0, A.dist[(uint64_t)v * kBcB + lane], x, (uint32_t)u, v);
+      const bool t1 = tight_bits(du1, A.dist[(uint64_t)v * kBcB + lane + 32], x, (uint32_t)u, v);
+      const uint64_t m = ((uint64_t)__ballot_sync(0xffffffffu, t0) |
+                          ((uint64_t)__ballot_sync(0xffffffffu, t1) << 32)) & A.qmask;
+      if (lane == 0) A.dag[k] = m;
+    }
+  }
+}
+
+// Round r of sigma: (w, source) settles when no tight predecessor is still
+// unsettled (as of the round's start); sigma = the sum over its tight
+// predecessors, in in-CSR order.
+__global__ void bcw_sigma_k(BcwArgs A) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  bool any = false;
+  for (uint64_t w = gw; w < A.n; w += nw) {
+    const uint64_t dp = A.done_prev[w];
+    const uint64_t pend = A.reach[w] & ~dp;
+    if (!pend) {
+      if (lane == 0) A.done_next[w] = dp;
+      continue;
+    }
+    const uint32_t b = A.in_off[w], e = A.in_off[w + 1];
+    uint64_t notready = 0;
+    for (uint32_t k = b + lane; k < e; k += 32) {
+      const uint64_t tm = A.dag[A.in_to_out[k]] & pend;
+      if (tm) notready |= tm & ~A.done_prev[A.in_src[k]];
+    }
+    notready = ((uint64_t)__reduce_or_sync(0xffffffffu, (unsigned)(notready >> 32)) << 32) |
+               __reduce_or_sync(0xffffffffu, (unsigned)notready);
+    const uint64_t ready = pend & ~notready;
+    if (lane == 0) A.done_next[w] = dp | ready;
+    if (!ready) continue;
+    any = true;
+    double s0 = 0.0, s1 = 0.0;
+    for (uint32_t k0 = b; k0 < e; k0 += 8) {
+      uint32_t ul = 0;
+      uint64_t tl = 0;
+      if (lane < 8 && k0 + lane < e) {
+        tl = A.dag[A.in_to_out[k0 + lane]] & ready;
+        if (tl) ul = A.in_src[k0 + lane];
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint64_t tj = __shfl_sync(0xffffffffu, tl, j);
+        const uint32_t uj = __shfl_sync(0xffffffffu, ul, j);
+        if (tj) {
+          if ((tj >> lane) & 1ull) s0 += A.sigma[(uint64_t)uj * kBcB + lane];
+          if ((tj >> (lane + 32)) & 1ull) s1 += A.sigma[(uint64_t)uj * kBcB + lane + 32];
+        }
+      }
+    }
+    if ((ready >> lane) & 1ull) {
+      A.sigma[w * kBcB + lane] = s0;
+      A.round[w * kBcB + lane] = A.r;
+    }
+    if ((ready >> (lane + 32)) & 1ull) {
+      A.sigma[w * kBcB + lane + 32] = s1;
+      A.round[w * kBcB + lane + 32] = A.r;
+    }
+  }
+  if (lane == 0 && any) atomicOr(A.found, 1u);
+}
+
+__global__ void fill_u64_bc_k(unsigned long long* p, uint64_t n, unsigned long long v) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
 __global__ void inv_perm_k(const uint32_t* __restrict__ eid, uint64_t m, uint32_t* __restrict__ inv) {
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m;
        k += (uint64_t)gridDim.x * blockDim.x)
@@ -455,6 +642,112 @@ static void betweenness_batched(TopoImpl* t, const std::vector<uint32_t>& source
     for (int32_t lvl = L - 1; lvl >= 0; lvl--) {
       a.level = lvl;
       bc_backward_k<<<gw, kBlock, 0, s>>>(a);
+      UG_LAUNCH_CHECK();
+    }
+    bc_fold_k<<<grid_for(n), kBlock, 0, s>>>(delta.get(), d_src.get(), nq, n, d_out);
+    UG_LAUNCH_CHECK();
+  }
+}
+
+// Weighted betweenness over `sources`, 64 at a time, added into d_out;
+// w_out: the weights in out-CSR slot order.
+static void betweenness_weighted_batched(TopoImpl* t, const double* w_out,
+                                         const std::vector<uint32_t>& sources, double* d_out,
+                                         cudaStream_t s) {
+  const uint64_t n = t->n, m = t->m;
+  ensure_in(t, s);
+  Scratch<uint32_t> in_to_out(m ? m : 1, s);
+  if (m) {
+    Scratch<uint32_t> inv(m, s);
+    inv_perm_k<<<grid_for(m), kBlock, 0, s>>>(t->out.eid.get(), m, inv.get());
+    UG_LAUNCH_CHECK();
+    compose_k<<<grid_for(m), kBlock, 0, s>>>(t->in.eid.get(), inv.get(), m, in_to_out.get());
+    UG_LAUNCH_CHECK();
+  }
+  Scratch<unsigned long long> dist(n * kBcB, s);
+  Scratch<uint64_t> fl0(n, s), fl1(n, s), reach(n, s), dn0(n, s), dn1(n, s), dag(m ? m : 1, s);
+  Scratch<int32_t> round(n * kBcB, s);
+  Scratch<double> sigma(n * kBcB, s), delta(n * kBcB, s);
+  Scratch<uint32_t> d_src(kBcB, s);
+  Scratch<unsigned> found(1, s);
+  BcwArgs a;
+  a.out_off = t->out.off.get();
+  a.out_tgt = t->out.tgt.get();
+  a.w_out = w_out;
+  a.in_off = t->in.off.get();
+  a.in_src = t->in.tgt.get();
+  a.in_to_out = in_to_out.get();
+  a.n = n;
+  a.dist = dist.get();
+  a.dag = dag.get();
+  a.reach = reach.get();
+  a.sigma = sigma.get();
+  a.round = round.get();
+  a.found = found.get();
+  BcBatchArgs bk{};  // the backward pass of the unweighted batch, on rounds and the tight DAG
+  bk.out_off = t->out.off.get();
+  bk.out_tgt = t->out.tgt.get();
+  bk.n = n;
+  bk.hop = round.get();
+  bk.sigma = sigma.get();
+  bk.delta = delta.get();
+  bk.dag = dag.get();
+  const unsigned gw = grid_for(n * 32, kBlock, 148u * 8u);
+  auto read_found = [&]() {
+    unsigned f = 0;
+    UG_CUDA(cudaMemcpyAsync(&f, found.get(), 4, cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
+    return f;
+  };
+  for (size_t c0 = 0; c0 < sources.size(); c0 += kBcB) {
+    const uint32_t nq = (uint32_t)std::min<size_t>(kBcB, sources.size() - c0);
+    a.qmask = nq == 64 ? ~0ull : ((1ull << nq) - 1ull);
+    UG_CUDA(cudaMemcpyAsync(d_src.get(), sources.data() + c0, nq * 4, cudaMemcpyHostToDevice, s));
+    fill_u64_bc_k<<<grid_for(n * kBcB), kBlock, 0, s>>>(dist.get(), n * kBcB, kInfBits);
+    UG_LAUNCH_CHECK();
+    UG_CUDA(cudaMemsetAsync(fl0.get(), 0, n * 8, s));
+    UG_CUDA(cudaMemsetAsync(fl1.get(), 0, n * 8, s));
+    UG_CUDA(cudaMemsetAsync(dn0.get(), 0, n * 8, s));
+    UG_CUDA(cudaMemsetAsync(round.get(), 0xFF, n * kBcB * 4, s));
+    UG_CUDA(cudaMemsetAsync(sigma.get(), 0, n * kBcB * 8, s));
+    UG_CUDA(cudaMemsetAsync(delta.get(), 0, n * kBcB * 8, s));
+    bcw_seed_k<<<1, kBcB, 0, s>>>(d_src.get(), nq, dist.get(), fl0.get(), dn0.get(), round.get(),
+                                  sigma.get());
+    UG_LAUNCH_CHECK();
+    // distances
+    uint64_t* cur = fl0.get();
+    uint64_t* nxt = fl1.get();
+    while (true) {
+      a.flag_cur = cur;
+      a.flag_next = nxt;
+      UG_CUDA(cudaMemsetAsync(found.get(), 0, 4, s));
+      bcw_relax_k<<<gw, kBlock, 0, s>>>(a);
+      UG_LAUNCH_CHECK();
+      UG_CUDA(cudaMemsetAsync(cur, 0, n * 8, s));  // consumed
+      if (!read_found()) break;
+      std::swap(cur, nxt);
+    }
+    // tight DAG, then sigma by rounds
+    bcw_tight_k<<<gw, kBlock, 0, s>>>(a);
+    UG_LAUNCH_CHECK();
+    uint64_t* dprev = dn0.get();
+    uint64_t* dnext = dn1.get();
+    int32_t r = 0;
+    while (true) {
+      a.r = r + 1;
+      a.done_prev = dprev;
+      a.done_next = dnext;
+      UG_CUDA(cudaMemsetAsync(found.get(), 0, 4, s));
+      bcw_sigma_k<<<gw, kBlock, 0, s>>>(a);
+      UG_LAUNCH_CHECK();
+      if (!read_found()) break;
+      r++;
+      std::swap(dprev, dnext);
+    }
+    // backward over rounds, deepest first (round r's nodes have no successors)
+    for (int32_t lvl = r - 1; lvl >= 0; lvl--) {
+      bk.level = lvl;
+      bc_backward_k<<<gw, kBlock, 0, s>>>(bk);
       UG_LAUNCH_CHECK();
     }
     bc_fold_k<<<grid_for(n), kBlock, 0, s>>>(delta.get(), d_src.get(), nq, n, d_out);
@@ -588,6 +881,8 @@ void betweenness_run(TopoImpl* t, const double* d_weights, bool has_sample, doub
   }
   if (!d_weights) {
     betweenness_batched(t, sources, d_out, s);
+  } else if (kBatchedWeighted) {
+    betweenness_weighted_batched(t, w_out.get(), sources, d_out, s);
   } else {
   Scratch<double> acc(n, s);
   for (size_t c0 = 0; c0 < sources.size(); c0 += kSrcChunk) {
