@@ -86,3 +86,18 @@ def test_build_twice_identical():
     a = Topology.build(n, s, d).incoming()
     b = Topology.build(n, s, d).incoming()
     assert np.array_equal(a.targets, b.targets) and np.array_equal(a.edge_ids, b.edge_ids)
+
+
+def test_pool_keeps_freed_blocks_until_released():
+    """Freed device buffers stay cached in the pool (the next build maps
+    nothing new) until ursa_gpu_pool_release returns them to the driver."""
+    import ursa_b200
+    from ursa_b200 import Topology, gen
+
+    n, s, d = gen.rmat(16, 16, 9)
+    g = Topology.build(n, s, d)
+    g.prepare(transpose=True)
+    g.free()
+    assert ursa_b200.pool_cached_bytes(0) > 0
+    ursa_b200.pool_release(0)
+    assert ursa_b200.pool_cached_bytes(0) == 0
