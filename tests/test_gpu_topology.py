@@ -94,10 +94,15 @@ def test_pool_keeps_freed_blocks_until_released():
     import ursa_b200
     from ursa_b200 import Topology, gen
 
+    import torch
+
     n, s, d = gen.rmat(16, 16, 9)
     g = Topology.build(n, s, d)
     g.prepare(transpose=True)
     g.free()
-    assert ursa_b200.pool_cached_bytes(0) > 0
+    torch.cuda.synchronize()  # the frees are stream-ordered
+    before = ursa_b200.pool_cached_bytes(0)
+    assert before >= 8 * s.size  # at least the freed CSR arrays
     ursa_b200.pool_release(0)
-    assert ursa_b200.pool_cached_bytes(0) == 0
+    # chunks that still hold live buffers stay reserved; everything else went back
+    assert ursa_b200.pool_cached_bytes(0) < before
