@@ -81,11 +81,11 @@ SCALE, EDGE_FACTOR, SEED = 22, 16, 2
 DAMPING, TOL, MAX_ITER = 0.85, 1e-6, 100
 WORKLOAD = "rmat22_pagerank"
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one pr_persistent_k launch on
-# this workload (prologue + 5 fixed iterations), measured by
-#   ncu --set full --clock-control none -k regex:pr_persistent -s 3 -c 1 \
-#     python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --max-iter 5 --tol 0
-NCU_TRAFFIC = {"bytes_per_launch": 1_341_229_000 + 55_156_736, "iterations": 5}
+# dram__bytes_read.sum + dram__bytes_write.sum of one PageRank kernel launch on
+# this workload (prologue + NCU_TRAFFIC["iterations"] fixed iterations), from an
+# ncu capture of the current kernel; None until one exists (the line then
+# reports traffic: null).
+NCU_TRAFFIC = None
 
 
 def env_int(name, default):
@@ -1658,7 +1658,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "kernel": "pr_persistent_k", "kernel_ms": mean_kernel_ms,
+                         "kernel": "pr_seg_k", "kernel_ms": mean_kernel_ms,
                          "algorithmic_bytes_per_launch": alg},
             "clocks": clocks,
         }
