@@ -74,11 +74,11 @@ constexpr uint32_t kPadEid = 0xFFFFFFFFu;
 constexpr uint64_t kWaitLimitNs = 5000000000ull;  // 5 s per bounded wait
 // chunk kinds
 constexpr int kSeg8 = 0, kSeg2 = 1, kFar4 = 2, kFar1 = 3, kLight4 = 4, kLight1 = 5;
-// relative cost per slot (phase-A balance across CTAs): shared-memory
-// gathers are cheap, L2 gathers are not; a chunk's cost is
-// (slots * weight) / 16 + kCostChunk, which keeps the u32 prefix far from
-// overflow (R-MAT-24 totals ~ 6e7)
-constexpr uint32_t kCostSeg = 2, kCostFar = 7, kCostLight = 5, kCostChunk = 6;
+// Static share of the segment chunks per CTA: a chunk costs about one
+// dependent index load per two column blocks (plus a fixed part), whatever
+// its width (measured: a warp's time per chunk follows its chain of
+// dependent loads, not its slot count).
+constexpr uint32_t kCostSegBase = 10, kCostSegPerBlock = 4, kCostSegShort = 14;
 }  // namespace
 
 struct PrChunk {
@@ -94,6 +94,7 @@ struct PrPlan {
   uint32_t iso_lo = 0;  // rows [iso_lo, n) are isolated
   uint32_t S = 0;       // segments with 16-bit ids
   uint32_t n_slots = 0, n_chunks = 0, n_groups = 0, n_wide = 0;
+  uint32_t n_seg_chunks = 0;  // chunks [0, n_seg_chunks) are the segment groups
   uint32_t n16 = 0, n32 = 0;  // slots in ids16 / ids32
   uint32_t group_begin[kMaxGroups + 1] = {};
   int32_t group_slice[kMaxGroups] = {};
@@ -366,8 +367,9 @@ __global__ void chunk_shape_k(const GroupDesc* __restrict__ groups, int ng, uint
     chunks[c] = ch;
     size16[c] = g.type == 0 ? size : 0u;
     size32[c] = g.type == 0 ? 0u : size;
-    const uint32_t wk = g.type == 0 ? kCostSeg : (g.type == 1 ? kCostFar : kCostLight);
-    cost[c] = size * wk / 16 + kCostChunk;
+    // only the segment chunks are split statically; far and light chunks
+    // are taken dynamically (their cost entries are 0)
+    cost[c] = g.type != 0 ? 0u : (kind == kSeg8 ? kCostSegBase + kCostSegPerBlock * nblk : kCostSegShort);
   }
 }
 
@@ -460,6 +462,8 @@ struct PrArgs {
   uint64_t n;
   uint32_t H, zi_lo, iso_lo;
   uint32_t n_chunks, n_groups, n_wide;
+  uint32_t n_seg_chunks;    // [0, n_seg_chunks): segment chunks, split by cost;
+                            // [n_seg_chunks, n_chunks): far / light, dealt round-robin
   uint32_t group_begin[kMaxGroups + 1];
   int32_t group_slice[kMaxGroups];
   const PrChunk* __restrict__ chunks;
@@ -510,6 +514,7 @@ struct PrSmem {
   int last;
   uint32_t n_sub;
   unsigned ctr[kMaxGroups];
+  unsigned dctr;  // the block's position in its share of the far / light chunks
   uint32_t sub_begin[kMaxGroups], sub_end[kMaxGroups];
   int32_t sub_slice[kMaxGroups];
 };
@@ -598,25 +603,38 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
   s = t;
 }
 
-// Share gathers.  far: global; light: the segment-0 slice for ids below
-// kSegW, else global.
+// Share gathers.  far: global; light: the loaded slice when the id falls in
+// it (slo = the slice's first id, have = a slice is loaded), else global.
 __device__ __forceinline__ float g_far(const float* x, uint32_t v) { return x[v]; }
-__device__ __forceinline__ float g_light(const PrSmem& sm, const float* x, uint32_t v) {
-  return v < kSegW ? sm.x[v] : x[v];
+struct SliceView {
+  uint32_t slo;
+  bool have;
+};
+__device__ __forceinline__ float g_light(const PrSmem& sm, SliceView sv, const float* x, uint32_t v) {
+  return (sv.have && v - sv.slo < kSegW) ? sm.x[v - sv.slo] : x[v];
+}
+
+__device__ __forceinline__ void add8(float& s, float& c, const float (&v)[8], int n) {
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+    if (k < n) kahan_add(s, c, v[k]);
 }
 
 // 16-bit local ids, eight per lane per block, gathered from the slice in
-// shared memory (padding id kSegW reads the zero slot); the next block's ids
-// are loaded before this block's gathers.
+// shared memory (padding id kSegW reads the zero slot); two blocks ahead are
+// in flight while a block is gathered and summed.
 template <bool kW>
 __device__ __forceinline__ F2 sum_seg8(const PrArgs& a, const PrSmem& sm, PrChunk ch, int lane) {
   const uint4* p = reinterpret_cast<const uint4*>(a.ids16 + ch.base) + lane;
+  const uint4 pad = make_uint4(kSegW | (kSegW << 16), kSegW | (kSegW << 16), kSegW | (kSegW << 16),
+                               kSegW | (kSegW << 16));
+  const uint32_t nb = ch.nblk;
   float s = 0.f, c = 0.f;
-  uint4 nx = __ldcs(p);
-  for (uint32_t b = 0; b < ch.nblk; b++) {
-    const uint4 q = nx;
-    if (b + 1 < ch.nblk) nx = __ldcs(p + (b + 1) * 32);
-    const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+  uint4 q0 = __ldcs(p);
+  uint4 q1 = nb > 1 ? __ldcs(p + 32) : pad;
+  for (uint32_t b = 0; b < nb; b++) {
+    const uint4 q2 = b + 2 < nb ? __ldcs(p + (b + 2) * 32) : pad;
+    const uint32_t w4[4] = {q0.x, q0.y, q0.z, q0.w};
     float v[8];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -636,61 +654,70 @@ __device__ __forceinline__ F2 sum_seg8(const PrArgs& a, const PrSmem& sm, PrChun
       v[6] = __fmul_rn(v[6], w1.z);
       v[7] = __fmul_rn(v[7], w1.w);
     }
-#pragma unroll
-    for (int k = 0; k < 8; k++) kahan_add(s, c, v[k]);
+    add8(s, c, v, 8);
+    q0 = q1;
+    q1 = q2;
   }
   return F2{s, -c};
 }
 
-// 16-bit local ids, two per lane per block, two blocks per step.
+// 16-bit local ids, two per lane per block, at most 8 blocks: every block's
+// ids are loaded at once, then gathered.
 template <bool kW>
 __device__ __forceinline__ F2 sum_seg2(const PrArgs& a, const PrSmem& sm, PrChunk ch, int lane) {
   const uint32_t* p = reinterpret_cast<const uint32_t*>(a.ids16 + ch.base) + lane;
+  const uint32_t nb = ch.nblk;
+  uint32_t q[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) q[k] = (uint32_t)k < nb ? __ldcs(p + k * 32) : (kSegW | (kSegW << 16));
   float s = 0.f, c = 0.f;
-  for (uint32_t b = 0; b < ch.nblk; b += 2) {
-    const bool two = b + 1 < ch.nblk;
-    const uint32_t q0 = __ldcs(p + b * 32);
-    const uint32_t q1 = two ? __ldcs(p + (b + 1) * 32) : (kSegW | (kSegW << 16));
-    float v[4] = {sm.x[q0 & 0xFFFFu], sm.x[q0 >> 16], sm.x[q1 & 0xFFFFu], sm.x[q1 >> 16]};
+#pragma unroll
+  for (int h = 0; h < 2; h++) {  // two halves of four blocks: eight gathers each
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      v[2 * k] = sm.x[q[4 * h + k] & 0xFFFFu];
+      v[2 * k + 1] = sm.x[q[4 * h + k] >> 16];
+    }
     if (kW) {
-      const float2* wp = reinterpret_cast<const float2*>(a.w16 + ch.base) + (size_t)b * 32 + lane;
-      const float2 w0 = __ldcs(wp);
-      const float2 w1 = two ? __ldcs(wp + 32) : make_float2(0.f, 0.f);
-      v[0] = __fmul_rn(v[0], w0.x);
-      v[1] = __fmul_rn(v[1], w0.y);
-      v[2] = __fmul_rn(v[2], w1.x);
-      v[3] = __fmul_rn(v[3], w1.y);
+      const float2* wp = reinterpret_cast<const float2*>(a.w16 + ch.base) + lane;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const float2 w = (uint32_t)(4 * h + k) < nb ? __ldcs(wp + (4 * h + k) * 32) : make_float2(0.f, 0.f);
+        v[2 * k] = __fmul_rn(v[2 * k], w.x);
+        v[2 * k + 1] = __fmul_rn(v[2 * k + 1], w.y);
+      }
     }
-    kahan_add(s, c, v[0]);
-    kahan_add(s, c, v[1]);
-    if (two) {
-      kahan_add(s, c, v[2]);
-      kahan_add(s, c, v[3]);
-    }
+    const int left = (int)nb - 4 * h;
+    add8(s, c, v, left <= 0 ? 0 : (left >= 4 ? 8 : 2 * left));
   }
   return F2{s, -c};
 }
 
 // 32-bit ids, four per lane per block, two blocks per step (eight gathers in
-// flight); kLight selects the segment-0 slice for small ids.
+// flight) while the next two blocks' ids load; kLight uses the loaded slice
+// as a cache.
 template <bool kW, bool kLight>
-__device__ __forceinline__ F2 sum_u32x4(const PrArgs& a, const PrSmem& sm, const float* x,
-                                        PrChunk ch, int lane) {
+__device__ __forceinline__ F2 sum_u32x4(const PrArgs& a, const PrSmem& sm, SliceView sv,
+                                        const float* x, PrChunk ch, int lane) {
   const uint4* p = reinterpret_cast<const uint4*>(a.ids32 + ch.base) + lane;
   const uint32_t pad = (uint32_t)a.n;
+  const uint4 pq = make_uint4(pad, pad, pad, pad);
+  const uint32_t nb = ch.nblk;
   float s = 0.f, c = 0.f;
-  for (uint32_t b = 0; b < ch.nblk; b += 2) {
-    const bool two = b + 1 < ch.nblk;
-    const uint4 q0 = __ldcs(p + b * 32);
-    const uint4 q1 = two ? __ldcs(p + (b + 1) * 32) : make_uint4(pad, pad, pad, pad);
-    const uint32_t id[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+  uint4 a0 = __ldcs(p);
+  uint4 a1 = nb > 1 ? __ldcs(p + 32) : pq;
+  for (uint32_t b = 0; b < nb; b += 2) {
+    const uint4 n0 = b + 2 < nb ? __ldcs(p + (b + 2) * 32) : pq;
+    const uint4 n1 = b + 3 < nb ? __ldcs(p + (b + 3) * 32) : pq;
+    const uint32_t id[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
     float v[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) v[k] = kLight ? g_light(sm, x, id[k]) : g_far(x, id[k]);
+    for (int k = 0; k < 8; k++) v[k] = kLight ? g_light(sm, sv, x, id[k]) : g_far(x, id[k]);
     if (kW) {
       const float4* wp = reinterpret_cast<const float4*>(a.w32 + ch.base) + (size_t)b * 32 + lane;
       const float4 w0 = __ldcs(wp);
-      const float4 w1 = two ? __ldcs(wp + 32) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 w1 = b + 1 < nb ? __ldcs(wp + 32) : make_float4(0.f, 0.f, 0.f, 0.f);
       v[0] = __fmul_rn(v[0], w0.x);
       v[1] = __fmul_rn(v[1], w0.y);
       v[2] = __fmul_rn(v[2], w0.z);
@@ -700,57 +727,60 @@ __device__ __forceinline__ F2 sum_u32x4(const PrArgs& a, const PrSmem& sm, const
       v[6] = __fmul_rn(v[6], w1.z);
       v[7] = __fmul_rn(v[7], w1.w);
     }
-#pragma unroll
-    for (int k = 0; k < 4; k++) kahan_add(s, c, v[k]);
-    if (two) {
-#pragma unroll
-      for (int k = 4; k < 8; k++) kahan_add(s, c, v[k]);
-    }
+    add8(s, c, v, b + 1 < nb ? 8 : 4);
+    a0 = n0;
+    a1 = n1;
   }
   return F2{s, -c};
 }
 
-// 32-bit ids, one per lane per block, four blocks per step.
+// 32-bit ids, one per lane per block, at most 8 blocks: every id is loaded
+// at once, then every share gathered.
 template <bool kW, bool kLight>
-__device__ __forceinline__ F2 sum_u32x1(const PrArgs& a, const PrSmem& sm, const float* x,
-                                        PrChunk ch, int lane) {
+__device__ __forceinline__ F2 sum_u32x1(const PrArgs& a, const PrSmem& sm, SliceView sv,
+                                        const float* x, PrChunk ch, int lane) {
   const uint32_t* p = a.ids32 + ch.base + lane;
-  float s = 0.f, c = 0.f;
-  for (uint32_t b = 0; b < ch.nblk; b += 4) {
-    uint32_t id[4];
+  const uint32_t nb = ch.nblk;
+  uint32_t id[8];
 #pragma unroll
-    for (int k = 0; k < 4; k++) id[k] = b + k < ch.nblk ? __ldcs(p + (b + k) * 32) : (uint32_t)a.n;
-    float v[4];
+  for (int k = 0; k < 8; k++) id[k] = (uint32_t)k < nb ? __ldcs(p + k * 32) : (uint32_t)a.n;
+  float v[8];
 #pragma unroll
-    for (int k = 0; k < 4; k++) v[k] = kLight ? g_light(sm, x, id[k]) : g_far(x, id[k]);
-    if (kW) {
+  for (int k = 0; k < 8; k++) v[k] = (uint32_t)k < nb ? (kLight ? g_light(sm, sv, x, id[k]) : g_far(x, id[k])) : 0.f;
+  if (kW) {
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        v[k] = __fmul_rn(v[k], b + k < ch.nblk ? __ldcs(a.w32 + ch.base + (size_t)(b + k) * 32 + lane)
-                                               : 0.f);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-      if (b + k < ch.nblk) kahan_add(s, c, v[k]);
+    for (int k = 0; k < 8; k++)
+      if ((uint32_t)k < nb) v[k] = __fmul_rn(v[k], __ldcs(a.w32 + ch.base + (size_t)k * 32 + lane));
   }
+  float s = 0.f, c = 0.f;
+  add8(s, c, v, (int)nb);
   return F2{s, -c};
+}
+
+// A chunk's descriptor and this lane's slot (loaded one chunk ahead).
+struct ChunkRef {
+  PrChunk ch;
+  uint32_t slot;
+};
+__device__ __forceinline__ ChunkRef chunk_ref(const PrArgs& a, uint32_t c, int lane) {
+  return ChunkRef{a.chunks[c], __ldg(a.chunk_slot + (size_t)c * 32 + lane)};
 }
 
 template <bool kW>
-__device__ __forceinline__ void run_chunk(const PrArgs& a, const PrSmem& sm, uint32_t c, int cur,
-                                          double base, Fx& f) {
+__device__ __forceinline__ void run_chunk(const PrArgs& a, const PrSmem& sm, SliceView sv, ChunkRef cr,
+                                          int cur, double base, Fx& f) {
   const int lane = threadIdx.x & 31;
-  const PrChunk ch = a.chunks[c];
-  const uint32_t slot = __ldg(a.chunk_slot + (size_t)c * 32 + lane);
+  const PrChunk ch = cr.ch;
+  const uint32_t slot = cr.slot;
   const float* x = a.x[cur];
   if (ch.kind == kLight4 || ch.kind == kLight1) {
     double old = 0.0, div = 0.0;
-    if (slot != kNoRow) {
-      old = a.rank[cur][slot];
+    if (slot != kNoRow) {  // the row was finished last iteration, maybe on another SM
+      old = __ldcg(a.rank[cur] + slot);
       div = row_divisor(a, slot);
     }
-    const F2 r = ch.kind == kLight4 ? sum_u32x4<kW, true>(a, sm, x, ch, lane)
-                                    : sum_u32x1<kW, true>(a, sm, x, ch, lane);
+    const F2 r = ch.kind == kLight4 ? sum_u32x4<kW, true>(a, sm, sv, x, ch, lane)
+                                    : sum_u32x1<kW, true>(a, sm, sv, x, ch, lane);
     if (slot != kNoRow) finish_row(a, slot, f2_value(r), old, div, base, cur, f);
     return;
   }
@@ -758,8 +788,8 @@ __device__ __forceinline__ void run_chunk(const PrArgs& a, const PrSmem& sm, uin
   switch (ch.kind) {
     case kSeg8: r = sum_seg8<kW>(a, sm, ch, lane); break;
     case kSeg2: r = sum_seg2<kW>(a, sm, ch, lane); break;
-    case kFar4: r = sum_u32x4<kW, false>(a, sm, x, ch, lane); break;
-    default: r = sum_u32x1<kW, false>(a, sm, x, ch, lane); break;
+    case kFar4: r = sum_u32x4<kW, false>(a, sm, sv, x, ch, lane); break;
+    default: r = sum_u32x1<kW, false>(a, sm, sv, x, ch, lane); break;
   }
   a.partial[slot] = r;
 }
@@ -862,14 +892,15 @@ __device__ __forceinline__ void sources_without_in_edges(const PrArgs& a, double
   }
 }
 
-// This block's contiguous range of the chunk list (by the cost prefix), cut
-// at group boundaries into sub-ranges, each with the slice it needs.
+// This block's contiguous range of the segment chunks (by the cost prefix),
+// cut at group boundaries into sub-ranges, each with the slice it needs.
 __device__ __forceinline__ void block_ranges(const PrArgs& a, PrSmem& sm) {
   if (threadIdx.x != 0) return;
-  const uint64_t total = a.n_chunks ? a.cost_prefix[a.n_chunks] : 0;
+  const uint32_t ns = a.n_seg_chunks;  // the statically split part
+  const uint64_t total = ns ? a.cost_prefix[ns] : 0;
   auto first_of = [&](uint32_t blk) -> uint32_t {  // first chunk whose start maps to >= blk
-    if (total == 0) return a.n_chunks;
-    uint32_t lo = 0, hi = a.n_chunks;
+    if (total == 0) return ns;
+    uint32_t lo = 0, hi = ns;
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
       if ((uint64_t)a.cost_prefix[mid] * gridDim.x / total < blk) lo = mid + 1; else hi = mid;
@@ -935,8 +966,9 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
     // base = (1-d)/n + d*dangling_mass/n   (pagerank.rs:79)
     const double base = __dadd_rn(__ddiv_rn(1.0 - a.damping, nf),
                                   __ddiv_rn(__dmul_rn(a.damping, dm), nf));
-    // ---- phase A: every chunk of this block's range
+    // ---- phase A, static part: this block's share of the segment chunks
     if (threadIdx.x < kMaxGroups) sm.ctr[threadIdx.x] = 0;
+    if (threadIdx.x == 0) sm.dctr = 0;
     __syncthreads();
     Fx f{0, 0};
     int loaded = -1;
@@ -948,42 +980,98 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
         load_slice(a, sm, a.x[cur], sl, phase);
         loaded = sl;
       }
+      const SliceView sv{(uint32_t)(loaded < 0 ? 0 : loaded) * kSegW, loaded >= 0};
       const uint32_t cb = sm.sub_begin[j], ce = sm.sub_end[j];
-      for (;;) {
-        uint32_t k = 0;
-        if (lane == 0) k = atomicAdd(&sm.ctr[j], 1u);
-        k = __shfl_sync(0xffffffffu, k, 0) + cb;
-        if (k >= ce) break;
-        run_chunk<kW>(a, sm, k, cur, base, f);
+      // the next chunk's descriptor and slot load while this one is summed
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&sm.ctr[j], 1u);
+      k = __shfl_sync(0xffffffffu, k, 0) + cb;
+      ChunkRef cr{};
+      if (k < ce) cr = chunk_ref(a, k, lane);
+      while (k < ce) {
+        uint32_t kn = 0;
+        if (lane == 0) kn = atomicAdd(&sm.ctr[j], 1u);
+        kn = __shfl_sync(0xffffffffu, kn, 0) + cb;
+        ChunkRef nx{};
+        if (kn < ce) nx = chunk_ref(a, kn, lane);
+        run_chunk<kW>(a, sm, sv, cr, cur, base, f);
+        k = kn;
+        cr = nx;
+      }
+    }
+    // ---- phase A, second part: far pieces, then light rows; light gathers
+    // use the slice this block has loaded as a cache
+    {
+      const SliceView sv{(uint32_t)(loaded < 0 ? 0 : loaded) * kSegW, loaded >= 0};
+      // the far and light chunks (sorted largest first) are dealt round-robin
+      // to the blocks, which balances them to one chunk, and the warps of a
+      // block take the block's share from a shared-memory counter
+      const uint32_t nd = a.n_chunks - a.n_seg_chunks, c0 = a.n_seg_chunks;
+      const uint32_t mine = blockIdx.x < nd ? (nd - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+      uint32_t j = 0;
+      if (lane == 0) j = atomicAdd(&sm.dctr, 1u);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      ChunkRef cr{};
+      if (j < mine) cr = chunk_ref(a, c0 + blockIdx.x + j * gridDim.x, lane);
+      while (j < mine) {
+        uint32_t jn = 0;
+        if (lane == 0) jn = atomicAdd(&sm.dctr, 1u);
+        jn = __shfl_sync(0xffffffffu, jn, 0);
+        ChunkRef nx{};
+        if (jn < mine) nx = chunk_ref(a, c0 + blockIdx.x + jn * gridDim.x, lane);
+        run_chunk<kW>(a, sm, sv, cr, cur, base, f);
+        j = jn;
+        cr = nx;
       }
     }
     grid_barrier(a.bar_count, a.bar_gen, gridDim.x, a.err, kWaitLimitNs);  // partials written
-    // ---- phase B: heavy rows combine their slots (slot order) and finish
-    for (uint32_t i = gwarp; i < a.n_wide; i += nwarps) {
-      const uint32_t r = a.wide_rows[i];
-      const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
-      F2 acc = f2_zero();
-      for (uint32_t k = s0 + lane; k < s1; k += 32) acc = f2_combine(acc, ldcg_f2(a.partial + k));
-      acc = warp_sum_f2(acc);
-      if (lane == 0)
-        finish_row(a, r, f2_value(acc), a.rank[cur][r], row_divisor(a, r), base, cur, f);
-    }
-    for (uint64_t r = gtid; r < a.H; r += nthr) {
-      const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
-      if (s1 - s0 > kWideSlots) continue;
-      const double old = a.rank[cur][r], div = row_divisor(a, r);
-      F2 acc = f2_zero();
-      uint32_t k = s0;
-      for (; k + 4 <= s1; k += 4) {
-        const F2 p0 = ldcg_f2(a.partial + k), p1 = ldcg_f2(a.partial + k + 1);
-        const F2 p2 = ldcg_f2(a.partial + k + 2), p3 = ldcg_f2(a.partial + k + 3);
-        acc = f2_combine(acc, p0);
-        acc = f2_combine(acc, p1);
-        acc = f2_combine(acc, p2);
-        acc = f2_combine(acc, p3);
+    // ---- phase B: heavy rows combine their slots (slot order) and finish.
+    // Rows are sorted by in-degree, heaviest first; consecutive rows go to
+    // consecutive blocks so the heavy ones spread over the GPU.
+    {
+      const uint32_t wrank = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // warps, block-interleaved
+      for (uint32_t i = wrank; i < a.n_wide; i += nwarps) {
+        const uint32_t r = a.wide_rows[i];
+        const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
+        // four independent streams per lane (slots lane + 32 j, j mod 4),
+        // combined in a fixed order
+        F2 acc[4] = {f2_zero(), f2_zero(), f2_zero(), f2_zero()};
+        uint32_t k = s0 + lane;
+        for (; k + 96 < s1; k += 128) {
+          const F2 p0 = ldcg_f2(a.partial + k), p1 = ldcg_f2(a.partial + k + 32);
+          const F2 p2 = ldcg_f2(a.partial + k + 64), p3 = ldcg_f2(a.partial + k + 96);
+          acc[0] = f2_combine(acc[0], p0);
+          acc[1] = f2_combine(acc[1], p1);
+          acc[2] = f2_combine(acc[2], p2);
+          acc[3] = f2_combine(acc[3], p3);
+        }
+        for (int j = 0; k < s1; k += 32, j++) acc[j & 3] = f2_combine(acc[j & 3], ldcg_f2(a.partial + k));
+        F2 t = warp_sum_f2(f2_combine(f2_combine(acc[0], acc[1]), f2_combine(acc[2], acc[3])));
+        if (lane == 0)
+          finish_row(a, r, f2_value(t), __ldcg(a.rank[cur] + r), row_divisor(a, r), base, cur, f);
       }
-      for (; k < s1; k++) acc = f2_combine(acc, ldcg_f2(a.partial + k));
-      finish_row(a, r, f2_value(acc), old, div, base, cur, f);
+      // the other heavy rows one per lane: a warp takes 32 consecutive rows
+      // (adjacent slot ranges: coalesced loads), and consecutive 32-row
+      // blocks go to consecutive blocks of the grid
+      const uint32_t n_rb = (a.H + 31) / 32;
+      for (uint32_t rb = wrank; rb < n_rb; rb += nwarps) {
+        const uint32_t r = rb * 32 + lane;
+        if (r >= a.H) continue;
+        const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
+        if (s1 - s0 > kWideSlots) continue;
+        const double old = __ldcg(a.rank[cur] + r), div = row_divisor(a, r);
+        F2 acc = f2_zero();
+        uint32_t k = s0;
+        for (; k + 8 <= s1; k += 8) {
+          F2 p[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) p[q] = ldcg_f2(a.partial + k + q);
+#pragma unroll
+          for (int q = 0; q < 8; q++) acc = f2_combine(acc, p[q]);
+        }
+        for (; k < s1; k++) acc = f2_combine(acc, ldcg_f2(a.partial + k));
+        finish_row(a, r, f2_value(acc), old, div, base, cur, f);
+      }
     }
     sources_without_in_edges(a, base, cur ^ 1, f);
     const Fx b = block_sum_fx(f, sm.red);
@@ -1164,10 +1252,10 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
     groups.push_back(g);
     n_chunks += (ie - ib + 31) / 32;
   };
-  for (uint32_t b = S; b-- > 1;) add_group(0, b, bb[b], bb[b + 1], (int)b);
+  for (uint32_t b = S; b-- > 0;) add_group(0, b, bb[b], bb[b + 1], (int)b);
+  plan->n_seg_chunks = n_chunks;  // the rest (far, then light) is taken dynamically
   if (H) add_group(1, S, bb[S], bb[S + 1], -1);
-  if (S >= 1) add_group(0, 0, bb[0], bb[1], 0);
-  add_group(2, 0, H, plan->zi_lo, 0);
+  add_group(2, 0, H, plan->zi_lo, -1);
   plan->n_groups = (uint32_t)groups.size();
   plan->group_begin[groups.size()] = n_chunks;
   plan->n_chunks = n_chunks;
@@ -1304,6 +1392,7 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   a.iso_lo = plan->iso_lo;
   a.n_chunks = plan->n_chunks;
   a.n_groups = plan->n_groups;
+  a.n_seg_chunks = plan->n_seg_chunks;
   a.n_wide = plan->n_wide;
   for (int g = 0; g <= kMaxGroups; g++) a.group_begin[g] = plan->group_begin[g];
   for (int g = 0; g < kMaxGroups; g++) a.group_slice[g] = plan->group_slice[g];
