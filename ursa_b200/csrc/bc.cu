@@ -293,7 +293,9 @@ __global__ void bc_forward_k(BcBatchArgs A) {
       if (lane < 8 && k0 + lane < e) {
         u = A.in_src[k0 + lane];
         f = A.front[u] & need;
-        if (f) A.dag[A.in_to_out[k0 + lane]] = f;
+        // an edge can be on several sources' DAGs at different levels; the
+        // warp owning v is the only writer of v's in-slots within a level
+        if (f) A.dag[A.in_to_out[k0 + lane]] |= f;
       }
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -711,6 +713,7 @@ static void betweenness_weighted_batched(TopoImpl* t, const double* w_out,
     UG_CUDA(cudaMemsetAsync(round.get(), 0xFF, n * kBcB * 4, s));
     UG_CUDA(cudaMemsetAsync(sigma.get(), 0, n * kBcB * 8, s));
     UG_CUDA(cudaMemsetAsync(delta.get(), 0, n * kBcB * 8, s));
+    if (m) UG_CUDA(cudaMemsetAsync(dag.get(), 0, m * 8, s));  // unreached nodes' slots stay 0
     bcw_seed_k<<<1, kBcB, 0, s>>>(d_src.get(), nq, dist.get(), fl0.get(), dn0.get(), round.get(),
                                   sigma.get());
     UG_LAUNCH_CHECK();
