@@ -880,15 +880,27 @@ __device__ __forceinline__ Fin barrier_totals(const PrArgs& a, int p, PrSmem& sm
 // Sources without in-edges (rows [zi_lo, iso_lo)): their rank is `rank`
 // (closed form, not stored per iteration); only the share they pass on is
 // written, and a dangling one (weighted, all out-weights 0) adds its rank to
-// the dangling mass.  A coalesced pass over all threads of the grid.
+// the dangling mass.  A coalesced pass over all threads of the grid, four
+// rows per thread per step so their divisor loads are in flight together.
 __device__ __forceinline__ void sources_without_in_edges(const PrArgs& a, double rank, int buf,
                                                          Fx& f) {
-  for (uint64_t u = a.zi_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u < a.iso_lo;
-       u += (uint64_t)gridDim.x * kPrBlock) {
-    const double div = row_divisor(a, u);
-    const bool dangling = !(div > 0.0);
-    a.x[buf][u] = dangling ? 0.f : (float)(rank / div);
-    if (dangling) f.dang += fx_of(rank);
+  const uint64_t stride = (uint64_t)gridDim.x * kPrBlock;
+  for (uint64_t u0 = a.zi_lo + (uint64_t)blockIdx.x * kPrBlock + threadIdx.x; u0 < a.iso_lo;
+       u0 += 4 * stride) {
+    double div[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint64_t u = u0 + q * stride;
+      div[q] = u < a.iso_lo ? row_divisor(a, u) : 1.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint64_t u = u0 + q * stride;
+      if (u >= a.iso_lo) break;
+      const bool dangling = !(div[q] > 0.0);
+      a.x[buf][u] = dangling ? 0.f : (float)(rank / div[q]);
+      if (dangling) f.dang += fx_of(rank);
+    }
   }
 }
 
@@ -1000,7 +1012,12 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
       }
     }
     // ---- phase A, second part: far pieces, then light rows; light gathers
-    // use the slice this block has loaded as a cache
+    // use the segment-0 slice (the most-gathered shares) as a cache
+    if (loaded != 0 && a.n_chunks > a.n_seg_chunks) {
+      __syncthreads();  // every warp is done with the previous slice
+      load_slice(a, sm, a.x[cur], 0, phase);
+      loaded = 0;
+    }
     {
       const SliceView sv{(uint32_t)(loaded < 0 ? 0 : loaded) * kSegW, loaded >= 0};
       // the far and light chunks (sorted largest first) are dealt round-robin
@@ -1024,15 +1041,49 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
         cr = nx;
       }
     }
+    // Work that does not need the partials runs before the barrier, where a
+    // block that finished early would otherwise wait: the sources without
+    // in-edges (they write next-iteration shares, which phase A never reads),
+    // and the loads of this warp's first phase-B rows (slot ranges, old
+    // ranks, divisors; none of them changes during phase A).
+    sources_without_in_edges(a, base, cur ^ 1, f);
+    const uint32_t wrank = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // warps, block-interleaved
+    const uint32_t n_rb = (a.H + 31) / 32;
+    uint32_t w_r = 0, w_s0 = 0, w_s1 = 0;
+    double w_old = 0.0, w_div = 0.0;
+    if (wrank < a.n_wide) {
+      w_r = a.wide_rows[wrank];
+      w_s0 = a.first_slot[w_r];
+      w_s1 = a.first_slot[w_r + 1];
+      w_old = __ldcg(a.rank[cur] + w_r);
+      w_div = row_divisor(a, w_r);
+    }
+    uint32_t n_s0 = 0, n_s1 = 0;
+    double n_old = 0.0, n_div = 0.0;
+    {
+      const uint32_t r = wrank * 32 + lane;
+      if (wrank < n_rb && r < a.H) {
+        n_s0 = a.first_slot[r];
+        n_s1 = a.first_slot[r + 1];
+        n_old = __ldcg(a.rank[cur] + r);
+        n_div = row_divisor(a, r);
+      }
+    }
     grid_barrier(a.bar_count, a.bar_gen, gridDim.x, a.err, kWaitLimitNs);  // partials written
     // ---- phase B: heavy rows combine their slots (slot order) and finish.
     // Rows are sorted by in-degree, heaviest first; consecutive rows go to
     // consecutive blocks so the heavy ones spread over the GPU.
     {
-      const uint32_t wrank = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // warps, block-interleaved
       for (uint32_t i = wrank; i < a.n_wide; i += nwarps) {
-        const uint32_t r = a.wide_rows[i];
-        const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
+        uint32_t r = w_r, s0 = w_s0, s1 = w_s1;
+        double old = w_old, div = w_div;
+        if (i != wrank) {  // beyond the first (prefetched) one
+          r = a.wide_rows[i];
+          s0 = a.first_slot[r];
+          s1 = a.first_slot[r + 1];
+          old = __ldcg(a.rank[cur] + r);
+          div = row_divisor(a, r);
+        }
         // four independent streams per lane (slots lane + 32 j, j mod 4),
         // combined in a fixed order
         F2 acc[4] = {f2_zero(), f2_zero(), f2_zero(), f2_zero()};
@@ -1047,19 +1098,23 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
         }
         for (int j = 0; k < s1; k += 32, j++) acc[j & 3] = f2_combine(acc[j & 3], ldcg_f2(a.partial + k));
         F2 t = warp_sum_f2(f2_combine(f2_combine(acc[0], acc[1]), f2_combine(acc[2], acc[3])));
-        if (lane == 0)
-          finish_row(a, r, f2_value(t), __ldcg(a.rank[cur] + r), row_divisor(a, r), base, cur, f);
+        if (lane == 0) finish_row(a, r, f2_value(t), old, div, base, cur, f);
       }
       // the other heavy rows one per lane: a warp takes 32 consecutive rows
       // (adjacent slot ranges: coalesced loads), and consecutive 32-row
       // blocks go to consecutive blocks of the grid
-      const uint32_t n_rb = (a.H + 31) / 32;
       for (uint32_t rb = wrank; rb < n_rb; rb += nwarps) {
         const uint32_t r = rb * 32 + lane;
         if (r >= a.H) continue;
-        const uint32_t s0 = a.first_slot[r], s1 = a.first_slot[r + 1];
+        uint32_t s0 = n_s0, s1 = n_s1;
+        double old = n_old, div = n_div;
+        if (rb != wrank) {
+          s0 = a.first_slot[r];
+          s1 = a.first_slot[r + 1];
+          old = __ldcg(a.rank[cur] + r);
+          div = row_divisor(a, r);
+        }
         if (s1 - s0 > kWideSlots) continue;
-        const double old = __ldcg(a.rank[cur] + r), div = row_divisor(a, r);
         F2 acc = f2_zero();
         uint32_t k = s0;
         for (; k + 8 <= s1; k += 8) {
@@ -1073,7 +1128,6 @@ __global__ void __launch_bounds__(kPrBlock, 1) pr_seg_k(PrArgs a) {
         finish_row(a, r, f2_value(acc), old, div, base, cur, f);
       }
     }
-    sources_without_in_edges(a, base, cur ^ 1, f);
     const Fx b = block_sum_fx(f, sm.red);
     if (threadIdx.x == 0) a.block_part[parity][blockIdx.x] = fx_pack(b.delta, b.dang);
     tot = barrier_totals(a, parity, sm, Fin{n_zi * fabs(base - prev_iso), n_iso * base});
