@@ -65,10 +65,12 @@ int ursa_gpu_set_device(int device);
 int ursa_gpu_thread_stream(int device, void **stream);
 /* Device memory: the library takes its device buffers (topologies, per-call
  * scratch) from the device's stream-ordered memory pool and keeps every
- * freed block cached in that pool, so repeated builds and calls never map
- * memory from the driver again.  These report and return that cache (an
- * extension with no counterpart in the reference): *cached = bytes the pool
- * holds but no buffer uses; release returns all of them to the driver
+ * freed block cached -- blocks of 4 MB and more at their own addresses, to
+ * be handed out again to requests that fit, smaller ones in that pool -- so
+ * repeated builds and calls neither map memory from the driver again nor pay
+ * the pool's cost of placing a large block.  These report and return that
+ * cache (an extension with no counterpart in the reference): *cached = bytes
+ * kept that no buffer uses; release returns all of them to the driver
  * (other processes and allocators can then use the memory). */
 int ursa_gpu_pool_cached_bytes(int device, uint64_t *cached);
 int ursa_gpu_pool_release(int device);

@@ -92,7 +92,7 @@ uint64_t pool_cached_bytes(int device) {
   uint64_t reserved = 0, used = 0;  // the attributes are 64-bit
   UG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
   UG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
-  return reserved > used ? (uint64_t)(reserved - used) : 0;
+  return (reserved > used ? (uint64_t)(reserved - used) : 0) + block_cache_idle_bytes(device);
 }
 
 int sm_count(int device) {
@@ -199,6 +199,7 @@ int ursa_gpu_pool_release(int device) {
     cudaMemPool_t pool;
     UG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     UG_CUDA(cudaSetDevice(device));
+    block_cache_flush(device);
     UG_CUDA(cudaDeviceSynchronize());  // frees still ordered on streams land in the pool first
     UG_CUDA(cudaMemPoolTrimTo(pool, 0));
   });

@@ -60,10 +60,18 @@ inline unsigned grid_for(uint64_t n, int block = kBlock, unsigned cap = 148u * 3
   return (unsigned)g;
 }
 
-// Stream-ordered device scratch from the device's default memory pool. The
-// pool keeps every freed block (its release threshold is raised to the
-// maximum once per device), so the steady state allocates nothing from the
-// driver.
+// Device blocks, stream-ordered.  Blocks of 4 MB and more are kept at their
+// addresses once freed and handed out again to later requests that fit (the
+// stream of the new owner waits on an event recorded where the block was
+// freed); smaller ones come from the device's default pool, which keeps every
+// freed block (its release threshold is raised to the maximum once per
+// device).  block_free never throws.
+void* block_alloc(size_t bytes, cudaStream_t s);
+void block_free(void* p, cudaStream_t s) noexcept;
+uint64_t block_cache_idle_bytes(int device);  // large blocks kept, none in use
+void block_cache_flush(int device);           // hands them back to the pool
+
+// Stream-ordered device scratch (block_alloc on the given stream, freed on it).
 template <class T>
 struct Scratch {
   T* p = nullptr;
@@ -75,10 +83,10 @@ struct Scratch {
     release();
     s = st;
     n = count;
-    if (count) UG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+    if (count) p = static_cast<T*>(block_alloc(count * sizeof(T), st));
   }
   void release() {
-    if (p) cudaFreeAsync(p, s);
+    if (p) block_free(p, s);
     p = nullptr;
     n = 0;
   }
@@ -94,8 +102,8 @@ struct Scratch {
   }
 };
 
-// Device allocation owned by a topology object, taken from the device's
-// stream-ordered pool on the building call's stream.  Every call that uses a
+// Device allocation owned by a topology object, taken with block_alloc on the
+// building call's stream.  Every call that uses a
 // topology has finished before it returns, so the free is ordered on the
 // per-thread default stream (always valid, whichever thread frees).
 template <class T>
@@ -106,10 +114,10 @@ struct DevArray {
   void alloc(size_t count, cudaStream_t s) {
     release();
     n = count;
-    if (count) UG_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), s));
+    if (count) p = static_cast<T*>(block_alloc(count * sizeof(T), s));
   }
   void release() {
-    if (p) cudaFreeAsync(p, cudaStreamPerThread);
+    if (p) block_free(p, cudaStreamPerThread);
     p = nullptr;
     n = 0;
   }

@@ -67,6 +67,7 @@ constexpr uint32_t kSegMax = 16;     // segments considered; ids >= kSegMax*kSeg
 constexpr uint32_t kBins = kSegMax + 1;
 constexpr uint32_t kPiece = 64;      // max edges per piece of a heavy row
 constexpr uint32_t kDirect = 32;     // rows with at most this many in-edges are light
+constexpr uint32_t kTile = 1024;     // heavy-row edges per grouping tile (one warp)
 constexpr uint32_t kWideSlots = 32;  // heavy rows with more slots are combined by a warp
 constexpr int kMaxGroups = kSegMax + 3;
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
@@ -192,31 +193,70 @@ __global__ void row_bounds_k(const uint32_t* __restrict__ deg, const uint32_t* _
   out[2] = (uint32_t)lo;
 }
 
-// Per heavy row, its in-edges per source segment (bins 0..kSegMax-1, bin
-// kSegMax = ids beyond); per bin, the edge total and the number of rows with
-// at least one edge there (for the choice of S).
-__global__ void seg_hist_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
-                           uint32_t H, uint32_t* __restrict__ cnt,
-                           unsigned long long* __restrict__ tot) {
+// Heavy rows' in-edges are grouped in tiles of up to kTile consecutive edges,
+// one warp per tile, so that a row of 10^5 edges spreads over ~100 warps.
+// tile_first[r] = row r's first tile (exclusive scan of these counts).
+__global__ void tile_count_k(const uint32_t* __restrict__ off, uint32_t H,
+                             uint32_t* __restrict__ tc) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < H; r += gridDim.x * blockDim.x)
+    tc[r] = (off[r + 1] - off[r] + kTile - 1) / kTile;
+}
+
+__global__ void tile_row_k(const uint32_t* __restrict__ tile_first, uint32_t H,
+                           uint32_t* __restrict__ tile_row) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < H; r += gridDim.x * blockDim.x)
+    for (uint32_t t = tile_first[r]; t < tile_first[r + 1]; t++) tile_row[t] = r;
+}
+
+// Per tile, its in-edges per source bin (bins 0..kSegMax-1 = kSegW-wide
+// slices of source ids, bin kSegMax = ids beyond).  *n_tiles is read on the
+// device (tile_first[H]).
+__global__ void tile_hist_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
+                            const uint32_t* __restrict__ tile_first,
+                            const uint32_t* __restrict__ tile_row,
+                            const uint32_t* __restrict__ n_tiles, uint32_t* __restrict__ th) {
   __shared__ uint32_t hist[kBlock / 32][kBins];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
-  unsigned long long my_edges = 0, my_pairs = 0;  // lane b: totals of bin b
-  for (uint32_t r = gw; r < H; r += nw) {
+  const uint32_t T = *n_tiles;
+  for (uint32_t t = gw; t < T; t += nw) {
+    const uint32_t r = tile_row[t];
+    const uint32_t e0 = off[r] + (t - tile_first[r]) * kTile;
+    const uint32_t e1 = min(e0 + kTile, off[r + 1]);
     if (lane < (int)kBins) hist[w][lane] = 0;
     __syncwarp();
-    for (uint32_t e = off[r] + lane; e < off[r + 1]; e += 32)
+    for (uint32_t e = e0 + lane; e < e1; e += 32)
       atomicAdd(&hist[w][min(src[e] / kSegW, kSegMax)], 1u);
     __syncwarp();
-    if (lane < (int)kBins) {
-      const uint32_t c = hist[w][lane];
-      cnt[(uint64_t)r * kBins + lane] = c;
-      my_edges += c;
-      my_pairs += c ? 1 : 0;
-    }
+    if (lane < (int)kBins) th[(uint64_t)t * kBins + lane] = hist[w][lane];
     __syncwarp();
   }
-  if (lane < (int)kBins && my_edges) {
+}
+
+// Per heavy row (one warp, lane b = bin b): its per-bin totals cnt[r][b] and,
+// in place, each tile's exclusive per-bin prefix within the row; per bin, the
+// edge total and the number of rows with an edge there (for the choice of S).
+__global__ void row_scan_k(const uint32_t* __restrict__ tile_first, uint32_t H,
+                           uint32_t* __restrict__ th, uint32_t* __restrict__ cnt,
+                           unsigned long long* __restrict__ tot) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  if (lane >= (int)kBins) return;
+  unsigned long long my_edges = 0, my_pairs = 0;
+  for (uint32_t r = gw; r < H; r += nw) {
+    uint32_t run = 0;
+    for (uint32_t t = tile_first[r]; t < tile_first[r + 1]; t++) {
+      uint32_t* p = th + (uint64_t)t * kBins + lane;
+      const uint32_t c = *p;
+      *p = run;
+      run += c;
+    }
+    cnt[(uint64_t)r * kBins + lane] = run;
+    my_edges += run;
+    my_pairs += run ? 1 : 0;
+  }
+  if (my_edges) {
     atomicAdd(&tot[lane], my_edges);
     atomicAdd(&tot[kBins + lane], my_pairs);
   }
@@ -248,28 +288,50 @@ __global__ void first_slot_k(const uint32_t* __restrict__ slot_base, uint32_t H,
     first[r] = r < H ? slot_base[(uint64_t)r * (S + 1)] : *total;
 }
 
-// Stable grouping of each heavy row's in-edges by merged segment (one warp
-// per row): segpre[r][b] = absolute start of bin b in the grouped arrays.
-__global__ void group_rows_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
-                             const uint32_t* __restrict__ eid, const uint32_t* __restrict__ cnt,
-                             uint32_t H, uint32_t S, uint32_t* __restrict__ segpre,
-                             uint32_t* __restrict__ gsrc, uint32_t* __restrict__ geid) {
+// segpre[r][b] = absolute start of row r's merged bin b (b in [0, S]) in the
+// grouped arrays; bins in order, starting at the row's first edge.
+__global__ void seg_prefix_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ cnt,
+                             uint32_t H, uint32_t S, uint32_t* __restrict__ segpre) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < H; r += gridDim.x * blockDim.x) {
+    uint32_t run = off[r];
+    for (uint32_t b = 0; b <= S; b++) {
+      segpre[(uint64_t)r * (S + 1) + b] = run;
+      run += merged_count(cnt, r, b, S);
+    }
+  }
+}
+
+// Stable grouping of each heavy row's in-edges by merged segment, one warp per
+// tile: the tile's edges of bin b go after the row's earlier tiles' edges of
+// bin b (th holds those per-tile exclusive prefixes).
+__global__ void group_tiles_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
+                              const uint32_t* __restrict__ eid,
+                              const uint32_t* __restrict__ tile_first,
+                              const uint32_t* __restrict__ tile_row,
+                              const uint32_t* __restrict__ n_tiles,
+                              const uint32_t* __restrict__ th, const uint32_t* __restrict__ segpre,
+                              uint32_t S, uint32_t* __restrict__ gsrc,
+                              uint32_t* __restrict__ geid) {
   __shared__ uint32_t cursor[kBlock / 32][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
   const unsigned lt = (1u << lane) - 1u;
-  for (uint32_t r = gw; r < H; r += nw) {
-    const uint32_t rb = off[r], re = off[r + 1];
-    uint32_t c = lane <= (int)S ? merged_count(cnt, r, (uint32_t)lane, S) : 0u;
-    uint32_t pre = c;  // inclusive warp scan
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, pre, o);
-      if (lane >= o) pre += t;
+  const uint32_t T = *n_tiles;
+  for (uint32_t t = gw; t < T; t += nw) {
+    const uint32_t r = tile_row[t];
+    const uint32_t rb = off[r] + (t - tile_first[r]) * kTile;
+    const uint32_t re = min(rb + kTile, off[r + 1]);
+    uint32_t c = 0;
+    if (lane <= (int)S) {
+      const uint32_t* p = th + (uint64_t)t * kBins;
+      c = segpre[(uint64_t)r * (S + 1) + lane];
+      if (lane < (int)S) {
+        c += p[lane];
+      } else {
+        for (uint32_t b = S; b < kBins; b++) c += p[b];
+      }
     }
-    pre -= c;
-    cursor[w][lane] = rb + pre;
-    if (lane <= (int)S) segpre[(uint64_t)r * (S + 1) + lane] = rb + pre;
+    cursor[w][lane] = c;
     __syncwarp();
     for (uint32_t e0 = rb; e0 < re; e0 += 32) {
       const uint32_t e = e0 + lane;
@@ -1238,11 +1300,25 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   // ---- heavy rows: per-segment counts and the number of 16-bit segments
   uint32_t S = 0;
   Scratch<uint32_t> cnt((uint64_t)(H ? H : 1) * kBins, s);
+  // grouping tiles: at most one per heavy row plus one per kTile edges
+  const uint64_t max_tiles = (uint64_t)H + m / kTile + 1;
+  Scratch<uint32_t> tile_first((uint64_t)H + 1, s);
+  Scratch<uint32_t> tile_row(H ? max_tiles : 1, s), th(H ? max_tiles * kBins : 1, s);
   if (H) {
+    tile_count_k<<<grid_for(H), kBlock, 0, s>>>(off.get(), H, tile_first.get());
+    UG_LAUNCH_CHECK();
+    UG_CUDA(cudaMemsetAsync(tile_first.get() + H, 0, sizeof(uint32_t), s));
+    exclusive_scan_u32(tile_first.get(), tile_first.get(), (uint64_t)H + 1, nullptr, s);
+    tile_row_k<<<grid_for(H), kBlock, 0, s>>>(tile_first.get(), H, tile_row.get());
+    UG_LAUNCH_CHECK();
+    tile_hist_k<<<grid_for(max_tiles * 32), kBlock, 0, s>>>(off.get(), src.get(), tile_first.get(),
+                                                            tile_row.get(), tile_first.get() + H,
+                                                            th.get());
+    UG_LAUNCH_CHECK();
     Scratch<unsigned long long> tot(2 * kBins, s);
     UG_CUDA(cudaMemsetAsync(tot.get(), 0, 2 * kBins * sizeof(unsigned long long), s));
-    seg_hist_k<<<grid_for((uint64_t)H * 32), kBlock, 0, s>>>(off.get(), src.get(), H, cnt.get(),
-                                                             tot.get());
+    row_scan_k<<<grid_for((uint64_t)H * 32), kBlock, 0, s>>>(tile_first.get(), H, th.get(),
+                                                             cnt.get(), tot.get());
     UG_LAUNCH_CHECK();
     unsigned long long h[2 * kBins];
     UG_CUDA(cudaMemcpyAsync(h, tot.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -1279,9 +1355,11 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   Scratch<uint32_t> prs(n_slots ? n_slots : 1, s);
   uint32_t bb[kSegMax + 2] = {0};
   if (H) {
-    group_rows_k<<<grid_for((uint64_t)H * 32), kBlock, 0, s>>>(off.get(), src.get(), eid.get(),
-                                                               cnt.get(), H, S, segpre.get(),
-                                                               gsrc.get(), geid.get());
+    seg_prefix_k<<<grid_for(H), kBlock, 0, s>>>(off.get(), cnt.get(), H, S, segpre.get());
+    UG_LAUNCH_CHECK();
+    group_tiles_k<<<grid_for(max_tiles * 32), kBlock, 0, s>>>(
+        off.get(), src.get(), eid.get(), tile_first.get(), tile_row.get(), tile_first.get() + H,
+        th.get(), segpre.get(), S, gsrc.get(), geid.get());
     UG_LAUNCH_CHECK();
     Scratch<uint32_t> key(n_slots ? n_slots : 1, s);
     piece_keys_k<<<grid_for((uint64_t)H * nb), kBlock, 0, s>>>(cnt.get(), slot_base.get(), H, S,

@@ -42,35 +42,77 @@ __device__ __forceinline__ uint32_t owner_of(const uint32_t* __restrict__ off, u
   return (uint32_t)lo;
 }
 
-// Visits every CSR slot k < m with its owning row: the grid walks the slots
-// in block-sized chunks, one thread finds the rows owning the chunk's first
-// and last slot, and each thread searches only between them.  body(k, u) is
-// called by the thread owning slot k.  Every thread of the block must call
-// this (it synchronises the block).
+// Largest u in [lo, n) with off[u] <= k, given off[lo] <= k; called by a
+// whole warp with the same arguments.  Two forward probes of 32 rows each
+// (one 128-byte load apiece) settle the usual case, where the owner is a few
+// short rows ahead of lo; a 32-ary search over [lo, n) settles the rest.
+__device__ __forceinline__ uint32_t warp_owner_from(const uint32_t* __restrict__ off, uint64_t n,
+                                                    uint64_t lo, uint64_t k) {
+  const int lane = threadIdx.x & 31;
+  for (int probe = 0; probe < 2; probe++) {
+    const uint64_t u = lo + 1 + (uint64_t)lane;
+    const bool ok = u < n && (uint64_t)off[u] <= k;
+    const unsigned msk = __ballot_sync(0xffffffffu, ok);
+    if (msk != 0xffffffffu) return (uint32_t)(lo + __popc(msk));  // ok is a prefix of the lanes
+    lo += 32;
+  }
+  uint64_t hi = n;  // the answer is in [lo, hi)
+  while (hi - lo > 1) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t p = lo + (uint64_t)(lane + 1) * step;
+    const bool ok = p < hi && (uint64_t)off[p] <= k;
+    const uint64_t c = (uint64_t)__popc(__ballot_sync(0xffffffffu, ok));
+    lo += c * step;
+    hi = (lo + step < hi) ? lo + step : hi;
+  }
+  return (uint32_t)lo;
+}
+
+// Visits every CSR slot k < m with its owning row.  Each block walks one
+// contiguous run of spans (kOwnerItems slots per thread); warp 0 finds the
+// rows owning a span's first and last slot by searching forward from the
+// previous span's owner, and each thread binary-searches only between them.
+// body(k, u) is called by the thread owning slot k.  Every thread of the
+// block must call this (it synchronises the block).
+constexpr int kOwnerItems = 4;
+
 template <class F>
 __device__ __forceinline__ void for_each_slot_owner(const uint32_t* __restrict__ off, uint64_t n,
                                                     uint64_t m, F&& body) {
   __shared__ uint32_t s_range[2];
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m; base += stride) {
-    if (threadIdx.x == 0) {
-      uint64_t last = base + blockDim.x - 1;
-      if (last >= m) last = m - 1;
-      s_range[0] = owner_of(off, n, base);
-      s_range[1] = owner_of(off, n, last);
+  const uint64_t span = (uint64_t)blockDim.x * kOwnerItems;
+  const uint64_t spans = (m + span - 1) / span;
+  const uint64_t per = (spans + gridDim.x - 1) / gridDim.x;
+  const uint64_t beg = min(m, (uint64_t)blockIdx.x * per * span);
+  const uint64_t end = min(m, beg + per * span);
+  uint64_t prev = 0;  // warp 0: a row with off[prev] <= the next span's first slot
+  for (uint64_t base = beg; base < end; base += span) {
+    const uint64_t last = min(base + span, end) - 1;
+    if (threadIdx.x < 32) {
+      const uint32_t lo = warp_owner_from(off, n, prev, base);
+      const uint32_t hi = warp_owner_from(off, n, lo, last);
+      if (threadIdx.x == 0) {
+        s_range[0] = lo;
+        s_range[1] = hi;
+      }
+      prev = hi;
     }
     __syncthreads();
-    const uint64_t k = base + threadIdx.x;
-    if (k < m) {
-      uint32_t lo = s_range[0], hi = s_range[1];  // answer in [lo, hi]
-      while (lo < hi) {
-        uint32_t mid = lo + ((hi - lo + 1) >> 1);
-        if ((uint64_t)off[mid] <= k)
-          lo = mid;
-        else
-          hi = mid - 1;
+    const uint32_t r0 = s_range[0], r1 = s_range[1];
+#pragma unroll
+    for (int j = 0; j < kOwnerItems; j++) {
+      const uint64_t k = base + (uint64_t)j * blockDim.x + threadIdx.x;
+      if (k <= last) {
+        uint32_t lo = r0, hi = r1;  // answer in [lo, hi]
+        while (lo < hi) {
+          const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+          if ((uint64_t)off[mid] <= k)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+        body(k, lo);
       }
-      body(k, lo);
     }
     __syncthreads();
   }
