@@ -129,6 +129,29 @@ def test_pagerank_weighted_zero_weights(orc):
     check(got, ref, a, b, 0.0)
 
 
+def test_pagerank_plain_then_weighted_on_one_topology(orc):
+    """The execution plan is cached on the topology and built without the
+    original edge ids until a weighted call needs them; the weighted call
+    then builds a plan with them, and later plain calls keep using it."""
+    from ursa_b200 import Topology, algo, gen
+
+    n, s, d = gen.rmat(16, 16, 7)
+    rng = np.random.default_rng(7)
+    w = rng.uniform(1.0, 10.0, s.size).astype(np.float32).astype(np.float64)
+    g = Topology.build(n, s, d)
+    o = orc.Topology(n, s, d)
+    ref_plain = orc.pagerank(o, 0.85, 20, 0.0)
+    ref_w = orc.pagerank_weighted(o, w, 0.85, 20, 0.0)
+    for weighted in (False, True, False, True):
+        if weighted:
+            got, ref = algo.pagerank_weighted(g, w, max_iter=20, tol=0.0), ref_w
+        else:
+            got, ref = algo.pagerank(g, max_iter=20, tol=0.0), ref_plain
+        l1, maxrel = errors(got, ref)
+        assert l1 <= L1_FIXED and maxrel <= MAXREL_FIXED, (weighted, l1, maxrel)
+    g.free()
+
+
 def test_pagerank_weighted_length_mismatch():
     from ursa_b200 import Topology, UrsaGpuError, algo
 

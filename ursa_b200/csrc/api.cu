@@ -44,12 +44,6 @@ __global__ void degree_dir_k(const uint32_t* __restrict__ a, const uint32_t* __r
   }
 }
 
-__global__ void check_range_k(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
-                              uint64_t m, uint64_t n, unsigned* __restrict__ bad) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    if ((uint64_t)a[i] >= n || (b && (uint64_t)b[i] >= n)) atomicOr(bad, 1u);
-}
 }  // namespace
 
 // degree.rs:12-30: out-, in- or total degree per node.
@@ -138,27 +132,20 @@ TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_
   t->device = device;
   t->n = n;
   t->m = m;
-  // The endpoint range check is read once at the end: the sort masks every
+  // The endpoint range check is done by the first radix pass of each sort
+  // (which reads every key) and read once at the end: the sort masks every
   // digit and its gathers index row positions, so out-of-range ids cannot
   // make it touch memory out of bounds -- the result is only discarded.
   Scratch<unsigned> bad(1, s);
   UG_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(unsigned), s));
-  if (m) {
-    check_range_k<<<grid_for(m), kBlock, 0, s>>>(d_src, nullptr, m, n, bad.get());
-    UG_LAUNCH_CHECK();
-  }
   // Out-CSR: rows by source; the destinations are only gathered in the last
   // radix pass, so they may still be arriving (dst_ready) until then.
-  build_csr(n, d_src, d_dst, m, t->out, s, dst_ready);
-  if (m) {
-    check_range_k<<<grid_for(m), kBlock, 0, s>>>(d_dst, nullptr, m, n, bad.get());
-    UG_LAUNCH_CHECK();
-  }
+  build_csr(n, d_src, d_dst, m, t->out, s, dst_ready, bad.get());
   // The endpoint columns are on the device in row order right now, so the
   // transpose is a second stable sort by destination -- the same in-CSR the
   // lazy reconstruction would produce (topology.rs:343-348), without
   // un-permuting the out-CSR later.
-  build_csr(n, d_dst, d_src, m, t->in, s);
+  build_csr(n, d_dst, d_src, m, t->in, s, nullptr, bad.get());
   t->has_in = true;
   unsigned hb = 0;
   UG_CUDA(cudaMemcpyAsync(&hb, bad.get(), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -287,7 +274,7 @@ uint64_t ursa_gpu_topo_device_bytes(const ursa_gpu_topo* t) {
   uint64_t b = 0;
   for (const DevCsr* c : {&i.out, &i.in}) b += (c->off.n + c->tgt.n + c->eid.n) * 4ull;
   b += (i.und_off.n + i.und_tgt.n + i.outdeg.n) * 4ull;
-  b += pr_plan_bytes(i.pr_plan);
+  b += pr_plan_bytes(i.pr_plan) + pr_plan_bytes(i.pr_plan_retired);
   return b;
 }
 

@@ -86,7 +86,7 @@ void csr_owners(const uint32_t* off, uint64_t n, uint64_t m, uint32_t* owner, cu
 }
 
 void build_csr(uint64_t n, const uint32_t* d_keys, const uint32_t* d_other, uint64_t m,
-               DevCsr& out, cudaStream_t s, cudaEvent_t other_ready) {
+               DevCsr& out, cudaStream_t s, cudaEvent_t other_ready, unsigned* bad) {
   out.off.alloc(n + 1, s);
   out.tgt.alloc(m, s);
   out.eid.alloc(m, s);
@@ -96,7 +96,7 @@ void build_csr(uint64_t n, const uint32_t* d_keys, const uint32_t* d_other, uint
   }
   Scratch<uint32_t> sorted_keys(m, s);
   radix_sort_pairs(d_keys, nullptr, m, bits_for(n ? n - 1 : 0), sorted_keys.get(), out.eid.get(),
-                   d_other, out.tgt.get(), s, other_ready);
+                   d_other, out.tgt.get(), s, other_ready, bad, n);
   offsets_from_sorted(sorted_keys.get(), m, n, out.off.get(), s);
 }
 

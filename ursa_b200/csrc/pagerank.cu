@@ -97,6 +97,7 @@ struct PrPlan {
   uint32_t n_slots = 0, n_chunks = 0, n_groups = 0, n_wide = 0;
   uint32_t n_seg_chunks = 0;  // chunks [0, n_seg_chunks) are the segment groups
   uint32_t n16 = 0, n32 = 0;  // slots in ids16 / ids32
+  bool with_eids = false;     // eid16 / eid32 built (weighted calls need them)
   uint32_t group_begin[kMaxGroups + 1] = {};
   int32_t group_slice[kMaxGroups] = {};
   DevArray<PrChunk> chunks;
@@ -163,7 +164,7 @@ __global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n,
     uint32_t u = old_of_new[i];
     uint32_t slot = in_off[u] + (uint32_t)(k - off_new[i]);
     src_new[k] = new_of_old[in_src[slot]];
-    eid_new[k] = in_eid[slot];
+    if (eid_new) eid_new[k] = in_eid[slot];
   });
 }
 
@@ -225,8 +226,17 @@ __global__ void tile_hist_k(const uint32_t* __restrict__ off, const uint32_t* __
     const uint32_t e1 = min(e0 + kTile, off[r + 1]);
     if (lane < (int)kBins) hist[w][lane] = 0;
     __syncwarp();
-    for (uint32_t e = e0 + lane; e < e1; e += 32)
-      atomicAdd(&hist[w][min(src[e] / kSegW, kSegMax)], 1u);
+    for (uint32_t e = e0 + lane; e < e1; e += 4 * 32) {
+      uint32_t b[4];  // four loads in flight before the counter updates
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint32_t ej = e + 32u * j;
+        b[j] = ej < e1 ? min(src[ej] / kSegW, kSegMax) : kBins;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (b[j] < kBins) atomicAdd(&hist[w][b[j]], 1u);
+    }
     __syncwarp();
     if (lane < (int)kBins) th[(uint64_t)t * kBins + lane] = hist[w][lane];
     __syncwarp();
@@ -239,27 +249,34 @@ __global__ void tile_hist_k(const uint32_t* __restrict__ off, const uint32_t* __
 __global__ void row_scan_k(const uint32_t* __restrict__ tile_first, uint32_t H,
                            uint32_t* __restrict__ th, uint32_t* __restrict__ cnt,
                            unsigned long long* __restrict__ tot) {
+  __shared__ unsigned long long s_tot[2 * kBins];
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  if (lane >= (int)kBins) return;
-  unsigned long long my_edges = 0, my_pairs = 0;
-  for (uint32_t r = gw; r < H; r += nw) {
-    uint32_t run = 0;
-    for (uint32_t t = tile_first[r]; t < tile_first[r + 1]; t++) {
-      uint32_t* p = th + (uint64_t)t * kBins + lane;
-      const uint32_t c = *p;
-      *p = run;
-      run += c;
+  for (int i = threadIdx.x; i < (int)(2 * kBins); i += blockDim.x) s_tot[i] = 0;
+  __syncthreads();
+  if (lane < (int)kBins) {
+    unsigned long long my_edges = 0, my_pairs = 0;
+    for (uint32_t r = gw; r < H; r += nw) {
+      uint32_t run = 0;
+      for (uint32_t t = tile_first[r]; t < tile_first[r + 1]; t++) {
+        uint32_t* p = th + (uint64_t)t * kBins + lane;
+        const uint32_t c = *p;
+        *p = run;
+        run += c;
+      }
+      cnt[(uint64_t)r * kBins + lane] = run;
+      my_edges += run;
+      my_pairs += run ? 1 : 0;
     }
-    cnt[(uint64_t)r * kBins + lane] = run;
-    my_edges += run;
-    my_pairs += run ? 1 : 0;
+    if (my_edges) {  // the block's totals first: few global atomics per address
+      atomicAdd(&s_tot[lane], my_edges);
+      atomicAdd(&s_tot[kBins + lane], my_pairs);
+    }
   }
-  if (my_edges) {
-    atomicAdd(&tot[lane], my_edges);
-    atomicAdd(&tot[kBins + lane], my_pairs);
-  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (int)(2 * kBins); i += blockDim.x)
+    if (s_tot[i]) atomicAdd(&tot[i], s_tot[i]);
 }
 
 // Count of heavy row r's edges in merged bin b of S+1 (b == S: far).
@@ -343,7 +360,7 @@ __global__ void group_tiles_k(const uint32_t* __restrict__ off, const uint32_t* 
       __syncwarp();
       if (valid) {
         gsrc[pos] = v;
-        geid[pos] = eid[e];
+        if (geid) geid[pos] = eid[e];
         if (lane == __ffs(peers) - 1) cursor[w][b] += __popc(peers);
       }
       __syncwarp();
@@ -468,7 +485,6 @@ __global__ void chunk_fill_k(const GroupDesc* __restrict__ groups, int ng, uint3
     const uint32_t V = ch.kind == kSeg8 ? 8u
                        : ch.kind == kSeg2 ? 2u
                        : (ch.kind == kFar4 || ch.kind == kLight4) ? 4u : 1u;
-    const uint32_t width = (uint32_t)ch.nblk * V;
     uint32_t len = 0, start = 0, sub = 0, slot_or_row = g.type == 2 ? kNoRow : n_slots;
     const uint32_t* ssrc = gsrc;
     const uint32_t* seid = geid;
@@ -491,17 +507,37 @@ __global__ void chunk_fill_k(const GroupDesc* __restrict__ groups, int ng, uint3
       }
     }
     chunk_slot[(uint64_t)c * 32 + lane] = slot_or_row;
-    for (uint32_t col = 0; col < width; col++) {
-      const uint64_t el = (uint64_t)ch.base + ((uint64_t)(col / V) * 32 + lane) * V + (col % V);
-      const bool have = col < len;
-      const uint32_t v = have ? ssrc[start + col] : 0u;
-      const uint32_t e = have ? seid[start + col] : kPadEid;
-      if (g.type == 0) {
-        ids16[el] = have ? (uint16_t)(v - sub) : (uint16_t)kSegW;
-        eid16[el] = e;
+    // a lane's V entries of a column block are contiguous (and V-aligned):
+    // gather them, then write them with one or two vector stores
+    const uint32_t pad = g.type == 0 ? kSegW : (uint32_t)n;
+    const bool with_eids = eid16 != nullptr;  // eid16 and eid32 are given together
+    for (uint32_t cb = 0; cb < ch.nblk; cb++) {
+      const uint64_t el = (uint64_t)ch.base + ((uint64_t)cb * 32 + lane) * V;
+      uint32_t vv[8], ee[8];
+#pragma unroll
+      for (uint32_t j = 0; j < 8; j++) {
+        const uint32_t col = cb * V + j;
+        const bool have = j < V && col < len;
+        vv[j] = have ? ssrc[start + col] - sub : pad;
+        ee[j] = have && with_eids ? seid[start + col] : kPadEid;
+      }
+      if (V == 8) {  // 16-bit ids
+        *reinterpret_cast<uint4*>(ids16 + el) =
+            make_uint4(vv[0] | vv[1] << 16, vv[2] | vv[3] << 16, vv[4] | vv[5] << 16,
+                       vv[6] | vv[7] << 16);
+        if (with_eids) {
+          *reinterpret_cast<uint4*>(eid16 + el) = make_uint4(ee[0], ee[1], ee[2], ee[3]);
+          *reinterpret_cast<uint4*>(eid16 + el + 4) = make_uint4(ee[4], ee[5], ee[6], ee[7]);
+        }
+      } else if (g.type == 0) {  // V == 2
+        *reinterpret_cast<uint32_t*>(ids16 + el) = vv[0] | vv[1] << 16;
+        if (with_eids) *reinterpret_cast<uint2*>(eid16 + el) = make_uint2(ee[0], ee[1]);
+      } else if (V == 4) {
+        *reinterpret_cast<uint4*>(ids32 + el) = make_uint4(vv[0], vv[1], vv[2], vv[3]);
+        if (with_eids) *reinterpret_cast<uint4*>(eid32 + el) = make_uint4(ee[0], ee[1], ee[2], ee[3]);
       } else {
-        ids32[el] = have ? v : (uint32_t)n;
-        eid32[el] = e;
+        ids32[el] = vv[0];
+        if (with_eids) eid32[el] = ee[0];
       }
     }
   }
@@ -1254,9 +1290,12 @@ T read1(const T* d, cudaStream_t s) {
 
 }  // namespace
 
-static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
+// with_eids: also the original edge id of every sliced-ELL entry (eid16 /
+// eid32), which only the weighted variant reads (to lay out its weights).
+static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s, bool with_eids) {
   const uint64_t n = t->n, m = t->m;
   auto* plan = new PrPlan();
+  plan->with_eids = with_eids;
   // ---- relabel by in-degree, highest first (stable: ties keep id order)
   {
     Scratch<uint32_t> key(n, s), key_sorted(n, s);
@@ -1275,7 +1314,8 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   UG_LAUNCH_CHECK();
   UG_CUDA(cudaMemsetAsync(deg.get() + n, 0, sizeof(uint32_t), s));
   exclusive_scan_u32(deg.get(), off.get(), n + 1, nullptr, s);
-  Scratch<uint32_t> src(m ? m : 1, s), eid(m ? m : 1, s);
+  Scratch<uint32_t> src(m ? m : 1, s), eid;
+  if (with_eids) eid.alloc(m ? m : 1, s);
   if (m) {
     relabel_copy_k<<<grid_for(m), kBlock, 0, s>>>(off.get(), n, m, plan->old_of_new.get(),
                                                    plan->new_of_old.get(), t->in.off.get(),
@@ -1350,7 +1390,8 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   // ---- heavy rows' edges grouped by bin; pieces sorted by (bin, length desc)
   const uint64_t m_heavy = H ? (uint64_t)read1(off.get() + H, s) : 0;
   Scratch<uint32_t> segpre((uint64_t)(H ? H : 1) * nb, s);
-  Scratch<uint32_t> gsrc(m_heavy ? m_heavy : 1, s), geid(m_heavy ? m_heavy : 1, s);
+  Scratch<uint32_t> gsrc(m_heavy ? m_heavy : 1, s), geid;
+  if (with_eids) geid.alloc(m_heavy ? m_heavy : 1, s);
   Scratch<uint32_t> skey(n_slots ? n_slots : 1, s), order(n_slots ? n_slots : 1, s);
   Scratch<uint32_t> prs(n_slots ? n_slots : 1, s);
   uint32_t bb[kSegMax + 2] = {0};
@@ -1417,9 +1458,9 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
     plan->n16 = n16;
     plan->n32 = n32;
     plan->ids16.alloc(n16 ? n16 : 8, s);
-    plan->eid16.alloc(n16 ? n16 : 8, s);
+    if (with_eids) plan->eid16.alloc(n16 ? n16 : 8, s);
     plan->ids32.alloc(n32 ? n32 : 4, s);
-    plan->eid32.alloc(n32 ? n32 : 4, s);
+    if (with_eids) plan->eid32.alloc(n32 ? n32 : 4, s);
     chunk_fill_k<<<grid_for((uint64_t)n_chunks * 32), kBlock, 0, s>>>(
         dg.get(), (int)groups.size(), n_chunks, plan->chunks.get(), skey.get(), order.get(),
         prs.get(), slot_base.get(), segpre.get(), gsrc.get(), geid.get(), off.get(), src.get(),
@@ -1445,10 +1486,16 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s) {
   return plan;
 }
 
-static PrPlan* ensure_pr_plan(TopoImpl* t, cudaStream_t s) {
+// The plan is cached on the topology; a weighted call on a plan built
+// without edge ids replaces it with one that has them (once).
+static PrPlan* ensure_pr_plan(TopoImpl* t, cudaStream_t s, bool with_eids) {
   ensure_in(t, s);
   std::lock_guard<std::mutex> g(t->mu);
-  if (!t->pr_plan) t->pr_plan = build_pr_plan(t, s);
+  if (t->pr_plan && with_eids && !t->pr_plan->with_eids) {
+    t->pr_plan_retired = t->pr_plan;  // at most once: plans with ids stay
+    t->pr_plan = nullptr;
+  }
+  if (!t->pr_plan) t->pr_plan = build_pr_plan(t, s, with_eids);
   return t->pr_plan;
 }
 
@@ -1476,8 +1523,8 @@ void pagerank_run(TopoImpl* t, const ursa_gpu_pagerank_params& p, const double* 
   const uint64_t n = t->n;
   if (stats) *stats = ursa_gpu_pagerank_stats{0, 0.0, 0.0};
   if (n == 0) return;
-  PrPlan* plan = ensure_pr_plan(t, s);
   const bool weighted = d_weights != nullptr;
+  PrPlan* plan = ensure_pr_plan(t, s, weighted);
   const int G = weighted ? pr_grid<true>(t->device) : pr_grid<false>(t->device);
   const size_t smem = pr_smem_bytes();
 

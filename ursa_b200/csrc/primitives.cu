@@ -118,10 +118,14 @@ void scan_impl(const T* in, T* out, uint64_t n, T* total, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------- radix sort
+// bad != nullptr: every key >= limit sets *bad (the caller's range check,
+// folded into the pass that reads the keys anyway).
 __global__ void __launch_bounds__(kBlock) radix_upsweep_k(const uint32_t* __restrict__ keys,
                                                           uint64_t n, int shift, uint32_t mask,
                                                           uint32_t* __restrict__ hist,
-                                                          uint32_t num_tiles) {
+                                                          uint32_t num_tiles,
+                                                          unsigned* __restrict__ bad,
+                                                          uint64_t limit) {
   __shared__ uint32_t cnt[kWarps][256];
   for (int i = threadIdx.x; i < kWarps * 256; i += kBlock) (&cnt[0][0])[i] = 0;
   __syncthreads();
@@ -134,11 +138,16 @@ __global__ void __launch_bounds__(kBlock) radix_upsweep_k(const uint32_t* __rest
     const uint64_t idx = base + (uint64_t)i * kBlock + threadIdx.x;
     k[i] = idx < n ? __ldg(&keys[idx]) : 0u;
   }
+  bool out_of_range = false;
 #pragma unroll
   for (int i = 0; i < kRadixItems; i++) {
     const uint64_t idx = base + (uint64_t)i * kBlock + threadIdx.x;
-    if (idx < n) atomicAdd(&cnt[w][(k[i] >> shift) & mask], 1u);
+    if (idx < n) {
+      atomicAdd(&cnt[w][(k[i] >> shift) & mask], 1u);
+      out_of_range |= (uint64_t)k[i] >= limit;
+    }
   }
+  if (bad && __any_sync(0xffffffffu, out_of_range) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
   __syncthreads();
   for (int d = threadIdx.x; d < 256; d += kBlock) {
     uint32_t s = 0;
@@ -258,7 +267,8 @@ void exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t*
 
 void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint64_t n, int key_bits,
                       uint32_t* keys_out, uint32_t* vals_out, const uint32_t* gather_src,
-                      uint32_t* gather_out, cudaStream_t s, cudaEvent_t gather_ready) {
+                      uint32_t* gather_out, cudaStream_t s, cudaEvent_t gather_ready,
+                      unsigned* bad, uint64_t limit) {
   UG_CHECK(n < (1ull << 32), URSA_GPU_EINVAL, "radix sort: more than 2^32-1 items");
   if (n == 0) return;
   int passes = key_bits <= 8 ? 1 : (key_bits + 7) / 8;
@@ -284,7 +294,8 @@ void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint64_t
     bool last = p == passes - 1;
     uint32_t* kout = last ? keys_out : kb[p & 1].get();
     uint32_t* vout = last ? vals_out : vb[p & 1].get();
-    radix_upsweep_k<<<num_tiles, kBlock, 0, s>>>(kin, n, shift, mask, hist.get(), num_tiles);
+    radix_upsweep_k<<<num_tiles, kBlock, 0, s>>>(kin, n, shift, mask, hist.get(), num_tiles,
+                                                 p == 0 ? bad : nullptr, limit);
     UG_LAUNCH_CHECK();
     exclusive_scan_u32(hist.get(), hist.get(), (uint64_t)256 * num_tiles, nullptr, s);
     if (last && gather_ready) UG_CUDA(cudaStreamWaitEvent(s, gather_ready, 0));

@@ -19,10 +19,14 @@ void exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t*
 // in the last pass (used to place the CSR targets next to their edge ids).
 // keys_out/vals_out must not alias the inputs.  n < 2^32.  gather_ready
 // (optional): an event the last pass waits for before it reads gather_src,
-// so gather_src may still be arriving while the earlier passes run.
+// so gather_src may still be arriving while the earlier passes run.  bad
+// (optional): set to nonzero if any key is >= limit (checked in the first
+// pass; the sort itself masks every digit, so such keys are sorted by their
+// low key_bits bits and the result is meant to be discarded).
 void radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint64_t n, int key_bits,
                       uint32_t* keys_out, uint32_t* vals_out, const uint32_t* gather_src,
-                      uint32_t* gather_out, cudaStream_t s, cudaEvent_t gather_ready = nullptr);
+                      uint32_t* gather_out, cudaStream_t s, cudaEvent_t gather_ready = nullptr,
+                      unsigned* bad = nullptr, uint64_t limit = 0);
 
 // offsets[u] = lower_bound(sorted_keys[0..m), u) for u in [0, n].
 void offsets_from_sorted(const uint32_t* sorted_keys, uint64_t m, uint64_t n, uint32_t* offsets,

@@ -45,17 +45,23 @@ struct TopoImpl {
     bool built = false;
   } ms_hubs[3];
   PrPlan* pr_plan = nullptr;
+  // a plan without edge ids, replaced by one with them for a weighted call;
+  // kept until the topology goes (a call on another thread may still use it)
+  PrPlan* pr_plan_retired = nullptr;
   std::mutex mu;
   ~TopoImpl() {
     if (pr_plan) pr_plan_free(pr_plan);
+    if (pr_plan_retired) pr_plan_free(pr_plan_retired);
   }
 };
 
 // Stable counting-sort CSR build from device endpoint arrays (keys group,
 // other is the paired endpoint); row order is kept inside each segment.
+// bad (optional): set nonzero if a key is >= n (the sort reads every key once
+// anyway; the result is then meant to be discarded).
 void build_csr(uint64_t n, const uint32_t* d_keys, const uint32_t* d_other, uint64_t m,
                DevCsr& out, cudaStream_t s,
-               cudaEvent_t other_ready = nullptr);
+               cudaEvent_t other_ready = nullptr, unsigned* bad = nullptr);
 // Lazily built parts; each call is a no-op once built.
 void ensure_in(TopoImpl* t, cudaStream_t s);
 void ensure_undirected(TopoImpl* t, cudaStream_t s);
