@@ -152,20 +152,75 @@ __global__ void relabel_maps_k(const uint32_t* __restrict__ old_of_new, uint64_t
   }
 }
 
-// Copy row old_of_new[i] of the in-CSR into new row i, relabelling sources.
-__global__ void relabel_copy_k(const uint32_t* __restrict__ off_new, uint64_t n, uint64_t m,
-                               const uint32_t* __restrict__ old_of_new,
-                               const uint32_t* __restrict__ new_of_old,
-                               const uint32_t* __restrict__ in_off,
-                               const uint32_t* __restrict__ in_src,
-                               const uint32_t* __restrict__ in_eid, uint32_t* __restrict__ src_new,
-                               uint32_t* __restrict__ eid_new) {
-  for_each_slot_owner(off_new, n, m, [&](uint64_t k, uint32_t i) {
-    uint32_t u = old_of_new[i];
-    uint32_t slot = in_off[u] + (uint32_t)(k - off_new[i]);
-    src_new[k] = new_of_old[in_src[slot]];
-    if (eid_new) eid_new[k] = in_eid[slot];
-  });
+// The in-CSR in the new labels (rows in execution order, sources relabelled).
+// Heavy rows: one warp per tile of up to kTile in-edges (tile t of row r
+// starts at edge t * kTile of the row), which also counts the tile's edges
+// per source bin (bins 0..kSegMax-1 = kSegW-wide slices of the new ids, bin
+// kSegMax = ids beyond).  *n_tiles is read on the device (tile_first[H]).
+__global__ void relabel_heavy_k(const uint32_t* __restrict__ off_new,
+                                const uint32_t* __restrict__ old_of_new,
+                                const uint32_t* __restrict__ new_of_old,
+                                const uint32_t* __restrict__ in_off,
+                                const uint32_t* __restrict__ in_src,
+                                const uint32_t* __restrict__ in_eid,
+                                const uint32_t* __restrict__ tile_first,
+                                const uint32_t* __restrict__ tile_row,
+                                const uint32_t* __restrict__ n_tiles,
+                                uint32_t* __restrict__ src_new, uint32_t* __restrict__ eid_new,
+                                uint32_t* __restrict__ th) {
+  __shared__ uint32_t hist[kBlock / 32][kBins];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
+  const uint32_t T = *n_tiles;
+  for (uint32_t t = gw; t < T; t += nw) {
+    const uint32_t r = tile_row[t];
+    const uint32_t first = (t - tile_first[r]) * kTile;
+    const uint32_t k0 = off_new[r] + first;
+    const uint32_t len = min(kTile, off_new[r + 1] - k0);
+    const uint32_t s0 = in_off[old_of_new[r]] + first;
+    if (lane < (int)kBins) hist[w][lane] = 0;
+    __syncwarp();
+    for (uint32_t x = lane; x < len; x += 4 * 32) {
+      uint32_t v[4];  // four gathers in flight before the stores and counts
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint32_t xq = x + 32u * q;
+        v[q] = xq < len ? new_of_old[in_src[s0 + xq]] : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint32_t xq = x + 32u * q;
+        if (xq < len) {
+          src_new[k0 + xq] = v[q];
+          if (eid_new) eid_new[k0 + xq] = in_eid[s0 + xq];
+          atomicAdd(&hist[w][min(v[q] / kSegW, kSegMax)], 1u);
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < (int)kBins) th[(uint64_t)t * kBins + lane] = hist[w][lane];
+    __syncwarp();
+  }
+}
+
+// Light rows [lo, hi) (at most kDirect in-edges each): one thread per row.
+__global__ void relabel_light_k(const uint32_t* __restrict__ off_new,
+                                const uint32_t* __restrict__ old_of_new,
+                                const uint32_t* __restrict__ new_of_old,
+                                const uint32_t* __restrict__ in_off,
+                                const uint32_t* __restrict__ in_src,
+                                const uint32_t* __restrict__ in_eid, uint32_t lo, uint32_t hi,
+                                uint32_t* __restrict__ src_new, uint32_t* __restrict__ eid_new) {
+  for (uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < hi;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t k0 = off_new[i], len = off_new[i + 1] - k0;
+    const uint32_t s0 = in_off[old_of_new[i]];
+#pragma unroll 4
+    for (uint32_t x = 0; x < len; x++) {
+      src_new[k0 + x] = new_of_old[in_src[s0 + x]];
+      if (eid_new) eid_new[k0 + x] = in_eid[s0 + x];
+    }
+  }
 }
 
 // Over the non-increasing in-degree sequence: out[0] = rows with in-degree >
@@ -209,40 +264,6 @@ __global__ void tile_row_k(const uint32_t* __restrict__ tile_first, uint32_t H,
     for (uint32_t t = tile_first[r]; t < tile_first[r + 1]; t++) tile_row[t] = r;
 }
 
-// Per tile, its in-edges per source bin (bins 0..kSegMax-1 = kSegW-wide
-// slices of source ids, bin kSegMax = ids beyond).  *n_tiles is read on the
-// device (tile_first[H]).
-__global__ void tile_hist_k(const uint32_t* __restrict__ off, const uint32_t* __restrict__ src,
-                            const uint32_t* __restrict__ tile_first,
-                            const uint32_t* __restrict__ tile_row,
-                            const uint32_t* __restrict__ n_tiles, uint32_t* __restrict__ th) {
-  __shared__ uint32_t hist[kBlock / 32][kBins];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
-  const uint32_t T = *n_tiles;
-  for (uint32_t t = gw; t < T; t += nw) {
-    const uint32_t r = tile_row[t];
-    const uint32_t e0 = off[r] + (t - tile_first[r]) * kTile;
-    const uint32_t e1 = min(e0 + kTile, off[r + 1]);
-    if (lane < (int)kBins) hist[w][lane] = 0;
-    __syncwarp();
-    for (uint32_t e = e0 + lane; e < e1; e += 4 * 32) {
-      uint32_t b[4];  // four loads in flight before the counter updates
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const uint32_t ej = e + 32u * j;
-        b[j] = ej < e1 ? min(src[ej] / kSegW, kSegMax) : kBins;
-      }
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if (b[j] < kBins) atomicAdd(&hist[w][b[j]], 1u);
-    }
-    __syncwarp();
-    if (lane < (int)kBins) th[(uint64_t)t * kBins + lane] = hist[w][lane];
-    __syncwarp();
-  }
-}
-
 // Per heavy row (one warp, lane b = bin b): its per-bin totals cnt[r][b] and,
 // in place, each tile's exclusive per-bin prefix within the row; per bin, the
 // edge total and the number of rows with an edge there (for the choice of S).
@@ -259,11 +280,16 @@ __global__ void row_scan_k(const uint32_t* __restrict__ tile_first, uint32_t H,
     unsigned long long my_edges = 0, my_pairs = 0;
     for (uint32_t r = gw; r < H; r += nw) {
       uint32_t run = 0;
-      for (uint32_t t = tile_first[r]; t < tile_first[r + 1]; t++) {
-        uint32_t* p = th + (uint64_t)t * kBins + lane;
-        const uint32_t c = *p;
-        *p = run;
-        run += c;
+      const uint32_t t1 = tile_first[r + 1];
+      for (uint32_t t = tile_first[r]; t < t1; t += 8) {
+        uint32_t c[8];  // eight tiles' counts in flight, then the running sum
+#pragma unroll
+        for (int q = 0; q < 8; q++) c[q] = t + q < t1 ? th[(uint64_t)(t + q) * kBins + lane] : 0u;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          if (t + q < t1) th[(uint64_t)(t + q) * kBins + lane] = run;
+          run += c[q];
+        }
       }
       cnt[(uint64_t)r * kBins + lane] = run;
       my_edges += run;
@@ -1314,15 +1340,6 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s, bool with_eids) {
   UG_LAUNCH_CHECK();
   UG_CUDA(cudaMemsetAsync(deg.get() + n, 0, sizeof(uint32_t), s));
   exclusive_scan_u32(deg.get(), off.get(), n + 1, nullptr, s);
-  Scratch<uint32_t> src(m ? m : 1, s), eid;
-  if (with_eids) eid.alloc(m ? m : 1, s);
-  if (m) {
-    relabel_copy_k<<<grid_for(m), kBlock, 0, s>>>(off.get(), n, m, plan->old_of_new.get(),
-                                                   plan->new_of_old.get(), t->in.off.get(),
-                                                   t->in.tgt.get(), t->in.eid.get(), src.get(),
-                                                   eid.get());
-    UG_LAUNCH_CHECK();
-  }
   // ---- row classes
   uint32_t bnd[3];
   {
@@ -1337,13 +1354,23 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s, bool with_eids) {
   plan->zi_lo = bnd[1];
   plan->iso_lo = bnd[2];
   UG_CHECK(H < (1u << 27), URSA_GPU_EINVAL, "pagerank: too many rows above the light-row degree");
-  // ---- heavy rows: per-segment counts and the number of 16-bit segments
+  // ---- the in-CSR in the new labels; heavy rows' per-segment counts and the
+  // number of 16-bit segments
   uint32_t S = 0;
   Scratch<uint32_t> cnt((uint64_t)(H ? H : 1) * kBins, s);
-  // grouping tiles: at most one per heavy row plus one per kTile edges
+  // tiles: at most one per heavy row plus one per kTile edges
   const uint64_t max_tiles = (uint64_t)H + m / kTile + 1;
   Scratch<uint32_t> tile_first((uint64_t)H + 1, s);
   Scratch<uint32_t> tile_row(H ? max_tiles : 1, s), th(H ? max_tiles * kBins : 1, s);
+  Scratch<uint32_t> src(m ? m : 1, s), eid;
+  if (with_eids) eid.alloc(m ? m : 1, s);
+  if (plan->zi_lo > H) {
+    relabel_light_k<<<grid_for(plan->zi_lo - H), kBlock, 0, s>>>(
+        off.get(), plan->old_of_new.get(), plan->new_of_old.get(), t->in.off.get(),
+        t->in.tgt.get(), t->in.eid.get(), H, plan->zi_lo, src.get(),
+        with_eids ? eid.get() : nullptr);
+    UG_LAUNCH_CHECK();
+  }
   if (H) {
     tile_count_k<<<grid_for(H), kBlock, 0, s>>>(off.get(), H, tile_first.get());
     UG_LAUNCH_CHECK();
@@ -1351,9 +1378,10 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s, bool with_eids) {
     exclusive_scan_u32(tile_first.get(), tile_first.get(), (uint64_t)H + 1, nullptr, s);
     tile_row_k<<<grid_for(H), kBlock, 0, s>>>(tile_first.get(), H, tile_row.get());
     UG_LAUNCH_CHECK();
-    tile_hist_k<<<grid_for(max_tiles * 32), kBlock, 0, s>>>(off.get(), src.get(), tile_first.get(),
-                                                            tile_row.get(), tile_first.get() + H,
-                                                            th.get());
+    relabel_heavy_k<<<grid_for(max_tiles * 32), kBlock, 0, s>>>(
+        off.get(), plan->old_of_new.get(), plan->new_of_old.get(), t->in.off.get(),
+        t->in.tgt.get(), t->in.eid.get(), tile_first.get(), tile_row.get(), tile_first.get() + H,
+        src.get(), with_eids ? eid.get() : nullptr, th.get());
     UG_LAUNCH_CHECK();
     Scratch<unsigned long long> tot(2 * kBins, s);
     UG_CUDA(cudaMemsetAsync(tot.get(), 0, 2 * kBins * sizeof(unsigned long long), s));
