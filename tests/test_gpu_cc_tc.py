@@ -90,6 +90,36 @@ def test_rmat18_exact(orc):
     assert np.array_equal(algo.connected_components_weak(g), canon(orc.connected_components_weak(o)))
 
 
+def test_triangles_long_oriented_lists_exact(orc):
+    """Oriented lists of every length class the counting kernel has: a
+    1,100-clique (its lowest-ranked member has 1,099 higher neighbours, above
+    the 1,024 a shared-memory table holds), a 400-clique (lists of 257..399),
+    hub stars and a sparse random part, all against the oracle."""
+    from ursa_b200 import algo
+
+    rng = np.random.default_rng(11)
+    src, dst = [], []
+    for base, k in ((0, 1100), (1100, 400)):
+        a, b = np.triu_indices(k, 1)
+        src.append(a + base)
+        dst.append(b + base)
+    n = 6000
+    m = 30_000
+    src.append(rng.integers(1500, n, m))
+    dst.append(rng.integers(1500, n, m))
+    for hub in (1500, 1501, 0):
+        leaves = rng.choice(np.arange(1500, n), 900, replace=False)
+        src.append(np.full(leaves.size, hub))
+        dst.append(leaves)
+    s = np.concatenate(src).astype(np.uint32)
+    d = np.concatenate(dst).astype(np.uint32)
+    g, o = _pair(orc, n, s, d)
+    got = algo.triangle_count(g)
+    assert np.array_equal(got, orc.triangle_count(o))
+    assert got[0] >= 1099 * 1098 // 2  # the clique's own triangles at node 0
+    assert np.array_equal(algo.clustering_coefficient(g), orc.clustering_coefficient(o))
+
+
 def test_rmat22_properties():
     """Full-size R-MAT-22: component labels are min-member ids (label[u] <= u,
     label[label[u]] == label[u]) and every edge joins one component;

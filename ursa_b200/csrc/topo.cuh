@@ -74,7 +74,6 @@ struct OrientedCsr {
   uint64_t mo = 0;
 };
 void orient_build(TopoImpl* t, OrientedCsr& o, cudaStream_t s);
-void triangle_count_oriented(const OrientedCsr& o, uint64_t n, uint32_t* d_tri, cudaStream_t s);
 void cc_weak_with_parent(TopoImpl* t, uint32_t* parent, uint32_t* d_out, cudaStream_t s);
 TopoImpl* topo_from_device(uint64_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m,
                            cudaStream_t s, int device, ursa_gpu_topo** holder,
