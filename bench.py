@@ -66,6 +66,7 @@ import argparse
 import ctypes as C
 import json
 import os
+import queue
 import statistics
 import subprocess
 import sys
@@ -1016,17 +1017,18 @@ SERVE_WORKLOAD = "serve_rmat24_uploads"
 SERVE_RATES = (1000, 2000, 5000, 10000, 20000, 50000)
 
 
-SERVE_MIX = {"shortest_path": 0.45, "bfs": 0.05, "hop2": 0.30, "pagerank": 0.20}
+SERVE_MIX = {"shortest_path": 0.45, "bfs": 0.002, "hop2": 0.348, "pagerank": 0.20}
 
 
 def serve_queries(n, rng, count):
     """(kind, a, b) with kind 0 = shortest_path(a, b), 1 = hop(a, k=2),
     2 = pagerank on the upload picked by b (a uniform draw), 3 = bfs from a
-    (Out).  The bfs/shortest_path half of the stream is 5% bfs: a bfs answer
-    is n i32 distances (67 MB at R-MAT-24), so bfs throughput is bound by the
-    host link (~800/s) whatever the GPU does."""
+    (Out).  0.2% of the stream is bfs: a bfs answer is n i32 distances (67 MB
+    at R-MAT-24), so bfs throughput is bound by the host link (~800/s) and
+    by the client's copy of each answer (~10 ms) whatever the GPU does; at
+    the sweep's top rate 0.2% is already 100 answers (6.7 GB) a second."""
     r = rng.random(count)
-    kind = np.where(r < 0.45, 0, np.where(r < 0.5, 3, np.where(r < 0.8, 1, 2)))
+    kind = np.where(r < 0.45, 0, np.where(r < 0.452, 3, np.where(r < 0.80, 1, 2)))
     a = rng.integers(0, n, count)
     b = rng.integers(0, n, count)
     return kind, a, b
@@ -1094,34 +1096,54 @@ def run_serve(args, rank, world):
                 break
         time.sleep(0.01)
 
+    def collector(tq, infos):
+        """Fetches results as they complete, keeping only the timings and
+        status (a bfs answer is n i32 values: holding thousands of them
+        would fill host memory); bfs answers land in one reused buffer."""
+        buf = torch.empty(n, dtype=torch.int32).pin_memory().numpy()
+        while True:
+            t = tq.get()
+            if t is None:
+                return
+            info = srv.result(t, timeout_s=600, out=buf)
+            info.result = None
+            infos.append(info)
+
     def drive(rate, count, seed):
         """Open-loop Poisson arrivals at `rate`; returns per-query infos."""
         rng = np.random.default_rng(seed)
         kind, a, b = serve_queries(n, rng, count)
         gaps = rng.exponential(1.0 / rate, count)
-        infos, tickets = [], []
+        infos = []
+        tq = queue.Queue()
+        ct = threading.Thread(target=collector, args=(tq, infos), daemon=True)
+        ct.start()
         t0 = time.perf_counter()
         t_next = t0
-        for i in range(count):
-            t_next += gaps[i]
-            while time.perf_counter() < t_next:
-                pass
-            if kind[i] == 0:
-                tickets.append(srv.shortest_path(int(a[i]), int(b[i])))
-            elif kind[i] == 1:
-                tickets.append(srv.hop(int(a[i]), 2))
-            elif kind[i] == 3:
-                tickets.append(srv.bfs(int(a[i]), 0))
-            else:
-                # pick and submit under the lock: the uploader removes an id
-                # from `live` (under it) before releasing the graph, and the
-                # submitted query keeps the graph until it finishes
-                with live_lock:
-                    gid = live[int(b[i]) % len(live)]
-                    tickets.append(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
-        offered = count / (time.perf_counter() - t0)
-        for t in tickets:
-            infos.append(srv.result(t, timeout_s=600))
+        try:
+            for i in range(count):
+                t_next += gaps[i]
+                while time.perf_counter() < t_next:
+                    pass
+                if kind[i] == 0:
+                    tq.put(srv.shortest_path(int(a[i]), int(b[i])))
+                elif kind[i] == 1:
+                    tq.put(srv.hop(int(a[i]), 2))
+                elif kind[i] == 3:
+                    tq.put(srv.bfs(int(a[i]), 0))
+                else:
+                    # pick and submit under the lock: the uploader removes an id
+                    # from `live` (under it) before releasing the graph, and the
+                    # submitted query keeps the graph until it finishes
+                    with live_lock:
+                        gid = live[int(b[i]) % len(live)]
+                        tq.put(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
+            offered = count / (time.perf_counter() - t0)
+        finally:
+            tq.put(None)
+            ct.join()
+        # infos come back in submission order (the collector waits on each
+        # ticket in turn), so kind[i] still describes infos[i]
         return infos, offered, kind
 
     def summarize(infos, kind):
@@ -1143,19 +1165,30 @@ def run_serve(args, rank, world):
         kind = np.full(count, k)
         a = rng.integers(0, n, count)
         b = rng.integers(0, n, count)
-        tickets = []
-        for i in range(count):
-            if k == 0:
-                tickets.append(srv.shortest_path(int(a[i]), int(b[i])))
-            elif k == 1:
-                tickets.append(srv.hop(int(a[i]), 2))
-            elif k == 3:
-                tickets.append(srv.bfs(int(a[i]), 0))
-            else:
-                with live_lock:
-                    gid = live[int(b[i]) % len(live)]
-                    tickets.append(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
-        infos = [srv.result(t, timeout_s=600) for t in tickets]
+        # four collecting threads, as the plain path has four calling threads
+        # (one query type, so the order of infos does not matter here)
+        infos = []
+        tq = queue.Queue()
+        cts = [threading.Thread(target=collector, args=(tq, infos), daemon=True) for _ in range(4)]
+        for ct in cts:
+            ct.start()
+        try:
+            for i in range(count):
+                if k == 0:
+                    tq.put(srv.shortest_path(int(a[i]), int(b[i])))
+                elif k == 1:
+                    tq.put(srv.hop(int(a[i]), 2))
+                elif k == 3:
+                    tq.put(srv.bfs(int(a[i]), 0))
+                else:
+                    with live_lock:
+                        gid = live[int(b[i]) % len(live)]
+                        tq.put(srv.pagerank(gid, max_iter=MAX_ITER, tol=TOL))
+        finally:
+            for _ in cts:
+                tq.put(None)
+            for ct in cts:
+                ct.join()
         return summarize(infos, kind)
 
     try:

@@ -438,7 +438,11 @@ typedef struct {
   uint64_t pr_max_nodes;           /* largest uploaded graph, in nodes */
   uint64_t hbm_reserve_bytes;      /* free HBM an upload must leave */
   uint64_t upload_budget_bytes;    /* device bytes of live uploads (0 = no cap) */
-  uint32_t bfs_lanes, bfs_slots;   /* bfs: lanes and queries per launch (<= 64) */
+  uint32_t bfs_lanes, bfs_slots;   /* bfs: lanes and queries per launch (<= 64).  Each
+                                      answer (n i32) waits in one of 2 x lanes x slots
+                                      pinned host buffers (allocated with the server)
+                                      until its result is fetched; with none free the
+                                      bfs lanes wait, the other lanes do not */
   uint64_t heartbeat_limit_ns;     /* slot kernels return after this long without a
                                       heartbeat (0 = 5 s) */
   uint64_t heartbeat_period_us;    /* the scheduler bumps the heartbeat this often

@@ -652,6 +652,7 @@ struct Request {
   ursa_gpu_query_info info{};
   std::vector<uint32_t> u32;  // path / reached nodes
   std::vector<double> f64;    // pagerank
+  uint32_t* pinned = nullptr; // bfs: the n distances, in a buffer of the server's pool
   bool done = false;
   bool cancel = false;
   std::shared_ptr<Upload> up;
@@ -704,6 +705,11 @@ struct Lane {
   unsigned* h_found = nullptr;
   std::vector<int32_t> b_row;  // per queued request: its row in the batch, -1 = out of range
   int32_t b_level = 0;         // last level enqueued
+  // a finished batch's n-sized answers are copied out by this thread (tens of
+  // ms per batch), so that the scheduler keeps serving the other lanes; the
+  // lane stays running until it is done (its device rows are reused)
+  std::thread harvester;
+  bool harvesting = false;
   int b_dir = 0;
   uint64_t b_qmask = 0;
 };
@@ -733,6 +739,13 @@ struct ursa_gpu_server {
   std::atomic<bool> stop{false};
   double last_heartbeat = 0.0;
   std::string fatal;  // a CUDA failure in the scheduler ends the server
+  // bfs answers (n i32 each) land in pinned host buffers at the host link's
+  // full rate: two batches' worth per bfs lane, allocated with the server.  A
+  // finished query holds one until its result is fetched; a batch waits for
+  // free buffers when clients fall behind (back-pressure on the bfs lanes
+  // only).
+  std::vector<uint32_t*> bfs_bufs, bfs_free;
+  std::condition_variable cv_bfs;
 };
 
 namespace ug {
@@ -1143,22 +1156,67 @@ void bfs_launch(ursa_gpu_server* S, Lane& L) {
 // Copies each query's distance row out (the server lock is not held).
 void bfs_harvest(ursa_gpu_server* S, Lane& L) {
   const uint64_t n = S->topo->n;
+  {  // one pool buffer per answer (the server's close ends the wait)
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (auto& rp : L.reqs) {
+      while (S->bfs_free.empty() && !S->stop.load())
+        S->cv_bfs.wait_for(lk, std::chrono::milliseconds(10));
+      if (S->bfs_free.empty()) throw Error(URSA_GPU_ECANCELED, "bfs: the server is closing");
+      rp->pinned = S->bfs_free.back();
+      S->bfs_free.pop_back();
+    }
+  }
   for (size_t i = 0; i < L.reqs.size(); i++) {
     Request& r = *L.reqs[i];
     r.info.status = URSA_GPU_OK;
     r.info.result_len = (int64_t)n;
     r.info.iterations = (uint32_t)L.b_level;
-    r.u32.resize(n);
     const int32_t row = L.b_row[i];
     if (row < 0) {
-      std::fill(r.u32.begin(), r.u32.end(), 0xFFFFFFFFu);
+      std::fill(r.pinned, r.pinned + n, 0xFFFFFFFFu);
       continue;
     }
     if (n)
-      UG_CUDA(cudaMemcpyAsync(r.u32.data(), L.b_dist.get() + (size_t)row * n, n * 4,
+      UG_CUDA(cudaMemcpyAsync(r.pinned, L.b_dist.get() + (size_t)row * n, n * 4,
                               cudaMemcpyDeviceToHost, L.copy));
   }
   UG_CUDA(cudaStreamSynchronize(L.copy));
+}
+
+void complete(ursa_gpu_server* S, const std::shared_ptr<Request>& r, double t);
+
+// The bfs lane's harvest thread: copies the finished batch's answers out,
+// then completes its requests and frees the lane under the server's lock.  A
+// CUDA failure fails the batch's requests and ends the server like a
+// scheduler failure does.
+void bfs_harvest_worker(ursa_gpu_server* S, Lane* L) {
+  std::string err;
+  try {
+    UG_CUDA(cudaSetDevice(S->device));
+    bfs_harvest(S, *L);
+  } catch (const std::exception& ex) {
+    err = ex.what();
+  }
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    const double t = now_us();
+    for (auto& r : L->reqs) {
+      if (!err.empty()) {
+        r->info.status = S->stop.load() ? URSA_GPU_ECANCELED : URSA_GPU_ECUDA;
+        r->info.result_len = 0;
+        if (r->pinned) S->bfs_free.push_back(r->pinned);
+        r->pinned = nullptr;
+      }
+      complete(S, r, t);
+    }
+    L->reqs.clear();
+    L->running = false;
+    L->harvesting = false;
+    L->last_use = t;
+    if (!err.empty() && !S->stop.load() && S->fatal.empty()) S->fatal = err;
+  }
+  S->cv_done.notify_all();
+  S->cv_sched.notify_all();
 }
 
 void complete(ursa_gpu_server* S, const std::shared_ptr<Request>& r, double t) {
@@ -1225,6 +1283,7 @@ void sched_loop(ursa_gpu_server* S) {
         if (L.kind == kLaneBfs) {
           // bfs: more levels, or harvest a finished batch; then refill
           if (L.running) {
+            if (L.harvesting) continue;  // its harvest thread frees the lane
             const cudaError_t e = cudaEventQuery(L.done);
             if (e == cudaErrorNotReady) continue;
             UG_CUDA(e);
@@ -1232,14 +1291,13 @@ void sched_loop(ursa_gpu_server* S) {
               bfs_enqueue_levels(S, L);
               continue;
             }
-            lk.unlock();
-            bfs_harvest(S, L);
-            lk.lock();
-            const double t = now_us();
-            for (auto& r : L.reqs) complete(S, r, t);
-            L.reqs.clear();
-            L.running = false;
+            // the previous harvest thread has set harvesting = false and
+            // released the lock, so this join returns at once
+            if (L.harvester.joinable()) L.harvester.join();
+            L.harvesting = true;
+            L.harvester = std::thread(bfs_harvest_worker, S, &L);
             progressed = true;
+            continue;
           }
           auto& bq = S->pending[kLaneBfs];
           while (!bq.empty() && L.reqs.size() < L.slots) {
@@ -1383,9 +1441,19 @@ int ursa_gpu_server_create(ursa_gpu_topo* resident, const ursa_gpu_server_config
       add(kLaneHop, cfg->hop_lanes, cfg->hop_slots);
       add(kLanePr, cfg->pr_lanes, cfg->pr_slots);
       add(kLaneBfs, cfg->bfs_lanes, cfg->bfs_slots);
+      if (cfg->bfs_lanes && S->topo->n) {
+        const uint64_t bufs = 2ull * cfg->bfs_lanes * cfg->bfs_slots;
+        for (uint64_t i = 0; i < bufs; i++) {
+          void* p = nullptr;
+          UG_CUDA(cudaHostAlloc(&p, S->topo->n * 4, cudaHostAllocDefault));
+          S->bfs_bufs.push_back(static_cast<uint32_t*>(p));
+        }
+        S->bfs_free = S->bfs_bufs;
+      }
     } catch (...) {
       for (auto& l : S->lanes) lane_raise_stop(*l);
       for (auto& l : S->lanes) lane_destroy(*l);
+      for (uint32_t* p : S->bfs_bufs) cudaFreeHost(p);
       throw;
     }
     ursa_gpu_server* raw = S.release();
@@ -1402,7 +1470,11 @@ void ursa_gpu_server_destroy(ursa_gpu_server* S) {
     S->stop.store(true);
   }
   S->cv_sched.notify_all();
+  S->cv_bfs.notify_all();
   if (S->sched.joinable()) S->sched.join();
+  for (auto& l : S->lanes)
+    if (l->harvester.joinable()) l->harvester.join();
+  for (uint32_t* p : S->bfs_bufs) cudaFreeHost(p);
   cudaSetDevice(S->device);
   for (auto& l : S->lanes) lane_raise_stop(*l);
   for (auto& l : S->lanes) lane_destroy(*l);
@@ -1592,22 +1664,35 @@ int ursa_gpu_server_result(ursa_gpu_server* S, uint64_t ticket, ursa_gpu_query_i
                            void* out, uint64_t cap_elems) {
   return guard([&] {
     UG_CHECK(S, URSA_GPU_EINVAL, "server is NULL");
-    std::lock_guard<std::mutex> g(S->mu);
-    auto it = S->reqs.find(ticket);
-    UG_CHECK(it != S->reqs.end(), URSA_GPU_EINVAL, "result: unknown ticket");
-    auto r = it->second;
-    UG_CHECK(r->done, URSA_GPU_ETIMEOUT, "result: the query has not completed");
-    if (info) *info = r->info;
-    const uint64_t len = r->info.type == URSA_GPU_QUERY_PAGERANK ? r->f64.size() : r->u32.size();
-    if (len > cap_elems) throw Error(URSA_GPU_ETRUNC, "result: buffer too small");
-    if (len) {
-      UG_CHECK(out, URSA_GPU_EINVAL, "result: out is NULL");
-      if (r->info.type == URSA_GPU_QUERY_PAGERANK)
-        std::memcpy(out, r->f64.data(), len * 8);
-      else
-        std::memcpy(out, r->u32.data(), len * 4);
+    std::shared_ptr<Request> r;
+    {
+      std::lock_guard<std::mutex> g(S->mu);
+      auto it = S->reqs.find(ticket);
+      UG_CHECK(it != S->reqs.end(), URSA_GPU_EINVAL, "result: unknown ticket");
+      r = it->second;
+      UG_CHECK(r->done, URSA_GPU_ETIMEOUT, "result: the query has not completed");
+      const uint64_t len = r->info.type == URSA_GPU_QUERY_PAGERANK ? r->f64.size()
+                           : r->pinned                              ? (uint64_t)r->info.result_len
+                                                                    : r->u32.size();
+      if (len > cap_elems) throw Error(URSA_GPU_ETRUNC, "result: buffer too small");
+      UG_CHECK(len == 0 || out, URSA_GPU_EINVAL, "result: out is NULL");
+      S->reqs.erase(it);  // the result is handed over once
     }
-    S->reqs.erase(it);  // the result is handed over once
+    // the copy runs without the server's lock (a bfs answer is n values)
+    if (info) *info = r->info;
+    if (r->info.type == URSA_GPU_QUERY_PAGERANK) {
+      if (!r->f64.empty()) std::memcpy(out, r->f64.data(), r->f64.size() * 8);
+    } else if (r->pinned) {
+      std::memcpy(out, r->pinned, (size_t)r->info.result_len * 4);
+      {
+        std::lock_guard<std::mutex> g(S->mu);
+        S->bfs_free.push_back(r->pinned);
+      }
+      r->pinned = nullptr;
+      S->cv_bfs.notify_all();
+    } else if (!r->u32.empty()) {
+      std::memcpy(out, r->u32.data(), r->u32.size() * 4);
+    }
   });
 }
 

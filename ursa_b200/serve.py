@@ -138,17 +138,20 @@ class Server:
         _lib.check(_lib.load().ursa_gpu_server_poll(self.handle, buf.ctypes.data, cap, C.byref(n)))
         return [int(x) for x in buf[: n.value]]
 
-    def result(self, ticket: int, timeout_s: float = 60.0) -> Completed:
-        """Waits for the query and takes its result (the ticket is then forgotten)."""
+    def result(self, ticket: int, timeout_s: float = 60.0, out: np.ndarray | None = None) -> Completed:
+        """Waits for the query and takes its result (the ticket is then forgotten).
+        `out` (optional): a contiguous array of the result's dtype with at least
+        info.result_len elements to receive it (e.g. one reused buffer for bfs
+        answers, n i32 each); the result is then a view of its first
+        result_len elements."""
         info = self.wait(ticket, timeout_s)
         L = _lib.load()
         n = max(int(info.result_len), 0)
-        if info.type == QUERY_PAGERANK:
-            out = np.empty(n, np.float64)
-        elif info.type == QUERY_BFS:
-            out = np.empty(n, np.int32)
+        dtype = np.float64 if info.type == QUERY_PAGERANK else (np.int32 if info.type == QUERY_BFS else np.uint32)
+        if out is not None and out.dtype == dtype and out.flags.c_contiguous and out.size >= n:
+            out = out[:n]
         else:
-            out = np.empty(n, np.uint32)
+            out = np.empty(n, dtype)
         _lib.check(L.ursa_gpu_server_result(self.handle, ticket, C.byref(info), out.ctypes.data if n else None, n))
         res = out
         if info.type == QUERY_SHORTEST_PATH and info.result_len < 0:
