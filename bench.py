@@ -1053,7 +1053,7 @@ def run_serve(args, rank, world):
     uoff = np.concatenate([[0], np.cumsum(uk)]).astype(np.int64)
     ups = [(int(un[i]), us[uoff[i]:uoff[i + 1]], ud[uoff[i]:uoff[i + 1]]) for i in range(len(un))]
     srv = Server(topo, path_lanes=4, path_slots=16, hop_lanes=4, hop_slots=16, pr_lanes=2, pr_slots=32,
-                 pr_max_nodes=65536, hbm_reserve_bytes=16 << 30, bfs_lanes=1, bfs_slots=16)
+                 pr_max_nodes=65536, hbm_reserve_bytes=16 << 30, bfs_lanes=2, bfs_slots=16)
     live, live_lock = [], threading.Lock()
     stop_up = threading.Event()
 
@@ -1327,7 +1327,7 @@ def run_serve(args, rank, world):
             "config": {"workload": SERVE_WORKLOAD, "resident_nodes": n, "resident_edges": m,
                        "uploads": "Poisson 200/s, 2 s lifetime, rmat_batch sizes",
                        "mix": SERVE_MIX,
-                       "lanes": {"shortest_path": [4, 16], "hop": [4, 16], "pagerank": [2, 32], "bfs": [1, 16]}},
+                       "lanes": {"shortest_path": [4, 16], "hop": [4, 16], "pagerank": [2, 32], "bfs": [2, 16]}},
             "closed_loop": closed,
             "sweep": sweep,
             "best_open_loop": {"rate_qps": best["rate_qps"], "completed_qps": best["completed_qps"]},
