@@ -140,9 +140,20 @@ __device__ __forceinline__ void append(uint32_t* Q, uint32_t* cnt, bool take, ui
   Q[base + __popc(mask & ((1u << lane) - 1u))] = v;
 }
 
+// Adds, per warp, the forward degrees of the nodes this round appended to the
+// next frontier (the next level's scout count, read with the frontier size).
+__device__ __forceinline__ void add_scout(DirView fwd, bool take, uint32_t v,
+                                          unsigned long long* __restrict__ scout) {
+  unsigned long long x = take ? (unsigned long long)dv_deg(fwd, v) : 0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if ((threadIdx.x & 31) == 0 && x) atomicAdd(scout, x);
+}
+
 __global__ void td_k(DirView d, const uint32_t* __restrict__ F, uint64_t f,
                      const uint64_t* __restrict__ pos, uint64_t T, int32_t* dist, int32_t level,
-                     uint32_t* __restrict__ N, uint32_t* __restrict__ cnt) {
+                     uint32_t* __restrict__ N, uint32_t* __restrict__ cnt,
+                     unsigned long long* __restrict__ scout) {
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t span = ((T + stride - 1) / stride) * stride;  // whole warps iterate together
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < span; e += stride) {
@@ -154,11 +165,13 @@ __global__ void td_k(DirView d, const uint32_t* __restrict__ F, uint64_t f,
       if (dist[v] < 0) take = atomicCAS(&dist[v], -1, level + 1) == -1;
     }
     append(N, cnt, take, v);
+    add_scout(d, take, v, scout);
   }
 }
 
-__global__ void bu_k(DirView rev, uint64_t n, int32_t* dist, int32_t level,
-                     uint32_t* __restrict__ N, uint32_t* __restrict__ cnt) {
+__global__ void bu_k(DirView rev, DirView fwd, uint64_t n, int32_t* dist, int32_t level,
+                     uint32_t* __restrict__ N, uint32_t* __restrict__ cnt,
+                     unsigned long long* __restrict__ scout) {
   uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t span = ((n + stride - 1) / stride) * stride;
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < span; v += stride) {
@@ -175,6 +188,7 @@ __global__ void bu_k(DirView rev, uint64_t n, int32_t* dist, int32_t level,
       }
     }
     append(N, cnt, take, (uint32_t)v);
+    add_scout(fwd, take, (uint32_t)v, scout);
   }
 }
 
@@ -284,31 +298,45 @@ void bfs_distances_run(TopoImpl* t, uint32_t source, int dir, int32_t* d_dist, c
   const double total_edges = (double)t->m * (dir == 2 ? 2.0 : 1.0);
   double edges_left = total_edges;
   const double alpha = 14.0, beta = 24.0;
+  // the frontier's out-edge total ("scout count"): the source's degree, then
+  // summed on the device by each level's kernel as it appends the next
+  // frontier, so a level costs one host read (frontier size and scout count)
+  Scratch<unsigned long long> scout(1, s);
+  uint64_t T = frontier_scan(fw, b.F.get(), f, b.pos.get(), s);
   while (f > 0) {
     UG_CUDA(cudaMemsetAsync(b.count.get(), 0, sizeof(uint32_t), s));
+    UG_CUDA(cudaMemsetAsync(scout.get(), 0, sizeof(unsigned long long), s));
     if (!bottom_up) {
-      uint64_t T = frontier_scan(fw, b.F.get(), f, b.pos.get(), s);
       if ((double)T > edges_left / alpha) {
         bottom_up = true;
       } else {
         if (T) {
+          // edge-balanced expansion: the frontier's degree prefix (its total is T)
+          fdeg_k<<<grid_for((uint64_t)f + 1), kBlock, 0, s>>>(fw, b.F.get(), f, b.pos.get());
+          UG_LAUNCH_CHECK();
+          exclusive_scan_u64(b.pos.get(), b.pos.get(), (uint64_t)f + 1, nullptr, s);
           td_k<<<grid_for(T, kBlock, 148u * 64u), kBlock, 0, s>>>(fw, b.F.get(), f, b.pos.get(), T,
                                                                    d_dist, level, b.N.get(),
-                                                                   b.count.get());
+                                                                   b.count.get(), scout.get());
           UG_LAUNCH_CHECK();
         }
         edges_left -= (double)T;
       }
     }
     if (bottom_up) {
-      bu_k<<<grid_for(n, kBlock, 148u * 64u), kBlock, 0, s>>>(rv, n, d_dist, level, b.N.get(),
-                                                               b.count.get());
+      bu_k<<<grid_for(n, kBlock, 148u * 64u), kBlock, 0, s>>>(rv, fw, n, d_dist, level, b.N.get(),
+                                                               b.count.get(), scout.get());
       UG_LAUNCH_CHECK();
     }
-    uint32_t next = read_u32(b.count.get(), s);
+    uint32_t next = 0;
+    unsigned long long t_next = 0;
+    UG_CUDA(cudaMemcpyAsync(&next, b.count.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaMemcpyAsync(&t_next, scout.get(), sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    UG_CUDA(cudaStreamSynchronize(s));
     if (bottom_up && (double)next < (double)n / beta && next < f) bottom_up = false;
     swap(b.F, b.N);
     f = next;
+    T = t_next;
     level++;
   }
 }
