@@ -66,6 +66,7 @@ def lib():
         L.orc_free.argtypes = [P]
         L.orc_connected_components_weak.argtypes = [P, P]
         L.orc_triangle_count.argtypes = [P, P]
+        L.orc_triangle_count_nodes.argtypes = [P, P, u64, P]
         L.orc_clustering_coefficient.argtypes = [P, P]
         L.orc_betweenness.argtypes = [P, i32, f64, i32, u64, P]
         L.orc_betweenness_weighted.argtypes = [P, P, i32, f64, i32, u64, P]
@@ -231,6 +232,16 @@ def connected_components_weak(t: Topology) -> np.ndarray:
 def triangle_count(t: Topology) -> np.ndarray:
     out = np.zeros(t.n, np.uint32)
     lib().orc_triangle_count(t._h, _p(out))
+    return out
+
+
+def triangle_count_nodes(t: Topology, nodes) -> np.ndarray:
+    """triangle_count's values for the given nodes only (the reference counts
+    each node on its own, triangle.rs:23-62)."""
+    nodes = np.ascontiguousarray(nodes, np.uint32)
+    assert nodes.size == 0 or int(nodes.max()) < t.n
+    out = np.zeros(nodes.size, np.uint32)
+    lib().orc_triangle_count_nodes(t._h, _p(nodes), nodes.size, _p(out))
     return out
 
 

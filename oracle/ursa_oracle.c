@@ -1043,6 +1043,41 @@ void orc_triangle_count(orc_topo *t, uint32_t *out) {
   par_ranges(t->n, par_threads_for(t->n + t->m), tc_range, &c);
 }
 
+/* The same per-node count (triangle.rs:23-62: node u, every neighbour
+ * a = N(u)[i], |N(u)[i+1..] & N(a)|) for the listed nodes only: the
+ * reference computes each node's count independently, so this is the
+ * reference's value for those nodes, at a cost a large graph can afford. */
+typedef struct {
+  const uint64_t *off;
+  const uint32_t *tg;
+  const uint32_t *nodes;
+  uint32_t *out;
+} tcn_ctx;
+
+static void tcn_range(void *p, uint64_t lo, uint64_t hi, int tid) {
+  tcn_ctx *c = (tcn_ctx *)p;
+  (void)tid;
+  for (uint64_t q = lo; q < hi; q++) {
+    const uint32_t u = c->nodes[q];
+    const uint32_t *nu = c->tg + c->off[u];
+    uint64_t du = c->off[u + 1] - c->off[u];
+    uint32_t count = 0;
+    for (uint64_t i = 0; i < du; i++) {
+      uint32_t a = nu[i];
+      count += intersection_count(nu + i + 1, du - i - 1, c->tg + c->off[a],
+                                  c->off[a + 1] - c->off[a]);
+    }
+    c->out[q] = count;
+  }
+}
+
+void orc_triangle_count_nodes(orc_topo *t, const uint32_t *nodes, uint64_t k, uint32_t *out) {
+  if (t->n == 0 || k == 0) return;
+  topo_undirected(t);
+  tcn_ctx c = {t->u_offsets, t->u_targets, nodes, out};
+  par_ranges(k, par_threads_for(k * 1024), tcn_range, &c);
+}
+
 void orc_clustering_coefficient(orc_topo *t, double *out) {
   uint64_t n = t->n;
   if (n == 0) return;

@@ -83,6 +83,8 @@ uint64_t orc_k_hop(orc_topo *t, const uint32_t *seeds, uint64_t n_seeds,
 void orc_free(void *p);
 void orc_connected_components_weak(orc_topo *t, uint32_t *out);
 void orc_triangle_count(orc_topo *t, uint32_t *out);
+/* triangle_count's per-node value for nodes[0..k) only (each node < n). */
+void orc_triangle_count_nodes(orc_topo *t, const uint32_t *nodes, uint64_t k, uint32_t *out);
 void orc_clustering_coefficient(orc_topo *t, double *out);
 void orc_betweenness(orc_topo *t, int has_sample, double sample, int has_seed,
                      uint64_t seed, double *out);

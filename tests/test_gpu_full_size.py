@@ -13,6 +13,8 @@ Bars (the same as the small-case tests):
     are mapped to each component's minimum member (components.rs:58-68);
   * BFS levels from seeded sources: exact (bfs.rs:18-42);
   * Dijkstra distances: bit-exact f64 (bfs.rs:126-166);
+  * triangle counts: bit-exact on a seeded sample of nodes (the reference
+    counts each node on its own, triangle.rs:23-62);
   * PageRank (pagerank.rs:98-169): the same iteration count as the oracle --
     a count that differs by one is accepted only where the oracle's L1
     residual at the earlier count lies within NEAR_TOL of tol (stated and
@@ -140,6 +142,27 @@ def test_c2_bfs_distances_multi_64_sources_exact(orc, c2):
         refs = list(ex.map(lambda x: orc.bfs_distances(o, x, "out"), srcs))
     for i, ref in enumerate(refs):
         assert np.array_equal(got[i], ref), srcs[i]
+
+
+def test_c2_triangle_counts_sampled_exact(orc, c2):
+    """Triangle counts at full size: the reference counts each node on its
+    own (triangle.rs:23-62), so the oracle restates it for a seeded sample of
+    nodes (all of them would take hours at this size): 4,000 nodes of degree
+    2..200 and 200 of degree 201..2,000, each count bit-exact."""
+    from ursa_b200 import algo
+
+    n, s, d, g, o = c2
+    got = algo.triangle_count(g)
+    deg = orc.degree(o, "both")
+    rng = np.random.default_rng(22)
+    low = np.flatnonzero((deg >= 2) & (deg <= 200))
+    mid = np.flatnonzero((deg > 200) & (deg <= 2000))
+    nodes = np.sort(np.concatenate([rng.choice(low, 4000, replace=False),
+                                    rng.choice(mid, 200, replace=False)]))
+    ref = orc.triangle_count_nodes(o, nodes)
+    assert ref.sum() > 0
+    assert np.array_equal(got[nodes], ref)
+    assert int(got.astype(np.int64).sum()) == 3 * 2_111_689_076
 
 
 def test_c3_pagerank_weighted(orc, c3):

@@ -273,6 +273,18 @@ def test_triangle_goldens(orc):
     assert list(T(orc.Topology(3, [0, 0, 1, 2, 0, 0], [1, 2, 2, 0, 0, 1]))) == [1, 1, 1]
 
 
+def test_triangle_count_nodes_equals_full_count(orc):
+    """The per-node restatement (used to check large graphs on a sample of
+    nodes) gives triangle_count's values for the listed nodes, in any order."""
+    rng = np.random.default_rng(5)
+    n, m = 2000, 30_000
+    t = orc.Topology(n, rng.integers(0, n, m).astype(np.uint32), rng.integers(0, n, m).astype(np.uint32))
+    full = orc.triangle_count(t)
+    nodes = rng.choice(n, 700, replace=False)
+    assert np.array_equal(orc.triangle_count_nodes(t, nodes), full[nodes])
+    assert orc.triangle_count_nodes(t, []).size == 0
+
+
 def test_clustering_goldens(orc):
     C = orc.clustering_coefficient  # clustering.rs:328-357
     assert list(C(orc.Topology(3, [0, 0, 1, 2], [1, 2, 2, 0]))) == [1.0, 1.0, 1.0]
