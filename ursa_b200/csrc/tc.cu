@@ -273,6 +273,135 @@ __global__ void __launch_bounds__(kWarps * 32) tc_middle_block_k(TcArgs a, uint3
   }
 }
 
+// ---- small graphs (the per-graph calls of a batch's plain path): the
+// rank relabelling, its two radix sorts and the host reads of the
+// middle-vertex path are a fixed cost of about a millisecond, more than the
+// whole count takes on a graph of a few tens of thousands of edges.  Below
+// kSmallEntries undirected CSR entries one kernel over the (degree, id)
+// orientation counts instead: a warp per vertex u puts N+(u) in a
+// shared-memory hash set (open addressing, load <= 1/2; longer lists are
+// searched by binary search in global memory) and streams the concatenation
+// of N+(v), v in N+(u), 32 lists at a time with lane p taking element p (its
+// list found by a warp scan of the lengths and a shuffle binary search); a
+// hit w is the triangle (u, v, w), credited to w at once and to v and u
+// through per-list counters in shared memory.
+constexpr uint64_t kSmallEntries = 1u << 18;
+constexpr int kSmThreads = 256;
+constexpr int kSmWarps = kSmThreads / 32;
+constexpr uint32_t kSmSlots = 2048;  // hash slots per warp
+constexpr uint32_t kSmHashMax = kSmSlots / 2;
+
+__global__ void __launch_bounds__(kSmThreads) count_small_k(const uint32_t* __restrict__ o_off,
+                                                          const uint32_t* __restrict__ o_tgt,
+                                                          uint64_t n, uint32_t* __restrict__ tri,
+                                                          unsigned long long* __restrict__ next) {
+  extern __shared__ uint32_t tc_sm[];
+  const uint32_t FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t* T = tc_sm + (size_t)w * kSmSlots;
+  uint32_t* cnt = tc_sm + (size_t)kSmWarps * kSmSlots + w * 32;
+  for (uint32_t i = lane; i < kSmSlots; i += 32) T[i] = kTcEmpty;
+  cnt[lane] = 0;
+  __syncwarp();
+  while (true) {
+    unsigned long long g = 0;
+    if (lane == 0) g = atomicAdd(next, (unsigned long long)kTcGrab);
+    g = __shfl_sync(FULL, g, 0);
+    if (g >= n) break;
+    const uint64_t g_end = g + kTcGrab < n ? g + kTcGrab : n;
+    for (uint64_t u = g; u < g_end; u++) {
+      const uint32_t ob = o_off[u], oe = o_off[u + 1], du = oe - ob;
+      if (du < 2) continue;  // u is the lowest vertex of no triangle
+      const bool hashed = du <= kSmHashMax;
+      uint32_t bits = 6;
+      while ((1u << bits) < 2 * du) bits++;
+      const uint32_t mask = (1u << bits) - 1;
+      if (hashed) {
+        for (uint32_t i = ob + lane; i < oe; i += 32) {
+          const uint32_t x = o_tgt[i];
+          uint32_t h = tc_hash(x, bits);
+          while (atomicCAS(&T[h], kTcEmpty, x) != kTcEmpty) h = (h + 1) & mask;
+        }
+        __syncwarp();
+      }
+      uint32_t cu = 0;
+      for (uint32_t vb = ob; vb < oe; vb += 32) {
+        const uint32_t i = vb + lane;
+        uint32_t v = 0, st = 0, len = 0;
+        if (i < oe) {
+          v = o_tgt[i];
+          st = o_off[v];
+          len = o_off[v + 1] - st;
+        }
+        uint32_t incl = len;  // inclusive scan of the list lengths
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(FULL, incl, o);
+          if (lane >= o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31);
+        for (uint32_t pb = 0; pb < total; pb += 32) {
+          const uint32_t p = pb + lane;
+          uint32_t j = 0;  // first list whose inclusive end exceeds p
+#pragma unroll
+          for (int step = 16; step >= 1; step >>= 1) {
+            const uint32_t t = __shfl_sync(FULL, incl, j + step - 1);
+            if (t <= p) j += step;
+          }
+          const uint32_t sj = __shfl_sync(FULL, st, j & 31);
+          const uint32_t ij = __shfl_sync(FULL, incl, j & 31);
+          const uint32_t lj = __shfl_sync(FULL, len, j & 31);
+          if (p < total) {
+            const uint32_t x = o_tgt[sj + (p - (ij - lj))];
+            bool hit = false;
+            if (hashed) {
+              uint32_t h = tc_hash(x, bits);
+              while (true) {
+                const uint32_t t = T[h];
+                if (t == x) {
+                  hit = true;
+                  break;
+                }
+                if (t == kTcEmpty) break;
+                h = (h + 1) & mask;
+              }
+            } else {
+              uint32_t lo = ob, hi = oe;
+              while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (o_tgt[mid] < x) lo = mid + 1; else hi = mid;
+              }
+              hit = lo < oe && o_tgt[lo] == x;
+            }
+            if (hit) {
+              atomicAdd(&tri[x], 1u);
+              atomicAdd(&cnt[j], 1u);
+            }
+          }
+        }
+        __syncwarp();
+        const uint32_t c = cnt[lane];
+        if (c) {
+          atomicAdd(&tri[v], c);
+          cu += c;
+          cnt[lane] = 0;
+        }
+        __syncwarp();
+      }
+      cu = __reduce_add_sync(FULL, cu);
+      if (lane == 0 && cu) atomicAdd(&tri[u], cu);
+      if (hashed) {
+        __syncwarp();
+        for (uint32_t k = lane; k <= mask; k += 32) T[k] = kTcEmpty;
+        __syncwarp();
+      }
+    }
+  }
+}
+
+
+size_t small_smem_bytes() { return ((size_t)kSmWarps * kSmSlots + kSmWarps * 32) * sizeof(uint32_t); }
+
 // ---- preparation: ranks, the rank-oriented CSR and its in-lists
 __global__ void und_degree_k(const uint32_t* __restrict__ off, uint64_t n, uint32_t* __restrict__ deg) {
   for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
@@ -459,6 +588,23 @@ void triangle_count_run(TopoImpl* t, uint32_t* d_tri, cudaStream_t s) {
   int dev = 0;
   UG_CUDA(cudaGetDevice(&dev));
   UG_CHECK(dev >= 0 && dev < 64, URSA_GPU_EINVAL, "device index out of range");
+  if (ms < kSmallEntries) {
+    OrientedCsr o;
+    orient_build(t, o, s);
+    if (o.mo) {
+      static std::mutex mu;
+      static int cache[64] = {0};
+      const int per_sm = tc_blocks_per_sm(count_small_k, kSmThreads, small_smem_bytes(), dev, cache, mu);
+      Scratch<unsigned long long> next(1, s);
+      UG_CUDA(cudaMemsetAsync(next.get(), 0, sizeof(unsigned long long), s));
+      count_small_k<<<per_sm * sm_count(dev), kSmThreads, small_smem_bytes(), s>>>(
+          o.off.get(), o.tgt.get(), n, d_tri, next.get());
+      UG_LAUNCH_CHECK();
+      count_launch();
+    }
+    UG_CUDA(cudaStreamSynchronize(s));  // o's buffers are released on return
+    return;
+  }
   // ranks by (undirected degree, id): a stable sort by degree
   Scratch<uint32_t> vertex_of(n, s), rank_of(n, s);
   {
