@@ -85,8 +85,8 @@ WORKLOAD = "rmat22_pagerank"
 # dram__bytes_read.sum + dram__bytes_write.sum of one PageRank kernel launch on
 # this workload (prologue + NCU_TRAFFIC["iterations"] iterations), from an ncu
 # --set full capture of pr_seg_k on this workload's own launch (converged in
-# 18 iterations): 3.872274 GB read + 0.757199 GB written.
-NCU_TRAFFIC = {"bytes_per_launch": 3_872_274_000 + 757_199_104, "iterations": 18}
+# 18 iterations): 3.588198 GB read + 0.466520 GB written.
+NCU_TRAFFIC = {"bytes_per_launch": 3_588_198_400 + 466_520_320, "iterations": 18}
 
 
 def env_int(name, default):

@@ -24,7 +24,7 @@
 //      - Heavy rows (in-degree > kDirect): each row's in-edges are grouped by
 //        source segment (stable, in-CSR order inside a segment) and cut into
 //        pieces of at most kPiece edges.  The first S segments (chosen per
-//        graph: the leading segments whose pieces average >= 3 edges) keep
+//        graph: the leading segments whose pieces average >= 5 edges) keep
 //        16-bit ids local to their segment; the remaining "far" sources keep
 //        32-bit ids.  Within a segment, pieces are sorted by length and packed
 //        32 to a chunk in sliced-ELL order: lane l's ids sit in column blocks
@@ -65,8 +65,9 @@ constexpr int kPrWarps = kPrBlock / 32;
 constexpr uint32_t kSegW = 49152;    // source ids per shared-memory slice (192 KB of f32 shares)
 constexpr uint32_t kSegMax = 16;     // segments considered; ids >= kSegMax*kSegW are far
 constexpr uint32_t kBins = kSegMax + 1;
-constexpr uint32_t kPiece = 64;      // max edges per piece of a heavy row
-constexpr uint32_t kDirect = 32;     // rows with at most this many in-edges are light
+constexpr uint32_t kPiece = 128;     // max edges per piece of a heavy row
+static_assert(kPiece <= 128, "kPiece - length (length >= 1) packs into 7 bits of a piece's sort key");
+constexpr uint32_t kDirect = 64;     // rows with at most this many in-edges are light
 constexpr uint32_t kTile = 1024;     // heavy-row edges per grouping tile (one warp)
 constexpr uint32_t kWideSlots = 32;  // heavy rows with more slots are combined by a warp
 constexpr int kMaxGroups = kSegMax + 3;
@@ -1391,9 +1392,9 @@ static PrPlan* build_pr_plan(TopoImpl* t, cudaStream_t s, bool with_eids) {
     unsigned long long h[2 * kBins];
     UG_CUDA(cudaMemcpyAsync(h, tot.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     UG_CUDA(cudaStreamSynchronize(s));
-    // a segment pays for its partial sums when its pieces average >= 3 edges
+    // a segment pays for its partial sums when its pieces average >= 5 edges
     while (S < kSegMax && (uint64_t)S * kSegW < plan->iso_lo && h[kBins + S] > 0 &&
-           h[S] >= 3ull * h[kBins + S])
+           h[S] >= 5ull * h[kBins + S])
       S++;
   }
   plan->S = S;
